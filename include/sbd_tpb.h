@@ -1,0 +1,168 @@
+/* sbd_tpb.h -- C ABI of the B200 tensor-product-basis (TPB) selected-basis diagonalization.
+ *
+ * One process, one GPU.  Inputs are an FCIDUMP-style Hamiltonian (core energy, one-electron
+ * integrals, 8-fold packed two-electron integrals) and sorted, duplicate-free alpha and beta
+ * occupation strings (uint64, bit p = spatial orbital p, L <= 64).  Outputs are the lowest
+ * eigenvalue, the CI vector in the reference's sign convention and determinant order
+ * (index Ia*nb + Ib), the orbital occupations and the spin-resolved 1- and 2-RDMs in the
+ * reference's layouts.  Every entry point returns an int status (SBD_TPB_OK = 0 or a negative
+ * SBD_TPB_ERR_* code); sbd_tpb_last_error() gives the message of the calling thread's last
+ * failure.  No entry point throws or exits the process.
+ *
+ * The reference interfaces each entry point replaces are cited as file:line inside ncsa/sbd-pub.
+ */
+#ifndef SBD_TPB_H
+#define SBD_TPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SBD_TPB_API __attribute__((visibility("default")))
+#else
+#define SBD_TPB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBD_TPB_OK 0
+#define SBD_TPB_ERR_INVALID (-1)       /* bad argument or inconsistent input */
+#define SBD_TPB_ERR_CUDA (-2)          /* CUDA runtime error (message says which call) */
+#define SBD_TPB_ERR_OOM (-3)           /* device allocation refused */
+#define SBD_TPB_ERR_NOT_CONVERGED (-4) /* Davidson stopped at max_it / max_time; result filled */
+#define SBD_TPB_ERR_STATE (-5)         /* call order: e.g. sigma before strings/Hamiltonian */
+#define SBD_TPB_ERR_IO (-6)            /* file could not be read or parsed */
+#define SBD_TPB_ERR_NO_DEVICE (-7)     /* no usable sm_100 device */
+
+/* Memory location of caller buffers passed to the vector entry points. */
+#define SBD_TPB_HOST 0
+#define SBD_TPB_DEVICE 1
+
+/* Table kinds for sbd_tpb_table_size / sbd_tpb_get_table. */
+#define SBD_TPB_SINGLES_ALPHA 0
+#define SBD_TPB_DOUBLES_ALPHA 1
+#define SBD_TPB_SINGLES_BETA 2
+#define SBD_TPB_DOUBLES_BETA 3
+
+/* Arithmetic of the solver. */
+#define SBD_TPB_FP64 0  /* FP64 vectors and sigma throughout (the plain path) */
+#define SBD_TPB_MIXED 1 /* FP32 CI/search vectors, FP32 sigma with split-BF16 tensor-core
+                           alpha-beta contraction, FP64 dots / Rayleigh-Ritz and a final FP64
+                           sigma for the reported energy and residual */
+
+/* Davidson correction. */
+#define SBD_TPB_PRECOND_DIAGONAL 0 /* t = r / (E0 - H_ii)  (tpb/davidson.h:858-868) */
+#define SBD_TPB_PRECOND_LEARNED 1  /* MLP correction, diagonal fallback when a step fails */
+
+typedef struct sbd_tpb_handle sbd_tpb_handle;
+
+/* Run parameters: the fields of sbd::tpb::SBD that matter on one rank (tpb/sbdiag.h:22-50). */
+typedef struct sbd_tpb_params {
+  int max_it;        /* --iteration: restarts of the Davidson subspace (default 1) */
+  int max_nb;        /* --block: subspace size (default 10) */
+  double eps;        /* --tolerance: residual norm (default 1e-4) */
+  double max_time;   /* --max_time in seconds (default 86400) */
+  int init;          /* --init: 0 = start from determinant 0 (the reference's HF start) */
+  int do_rdm;        /* --rdm: 0 = orbital occupations only, 1 = full 1/2-RDMs */
+  int precision;     /* SBD_TPB_FP64 or SBD_TPB_MIXED */
+  int preconditioner;/* SBD_TPB_PRECOND_* */
+  int verbose;       /* print the reference's " Davidson iteration" lines to stdout */
+  int device;        /* CUDA device ordinal used by sbd_tpb_diag */
+} sbd_tpb_params;
+
+/* Fills p with the reference defaults (tpb/sbdiag.h:22-50) and SBD_TPB_FP64 / diagonal. */
+SBD_TPB_API void sbd_tpb_default_params(sbd_tpb_params *p);
+
+/* Hamiltonian in FCIDUMP terms.  h1 is L*L row-major and symmetric; eri_packed is the 8-fold
+ * store of twoInt (basic/integrals.h:64-107): index a*(a+1)/2+b with a >= b over the pair
+ * indices ij = max(i,j)*(max(i,j)+1)/2 + min(i,j); length B*(B+1)/2, B = L*(L+1)/2. */
+typedef struct sbd_tpb_hamiltonian {
+  int norb;
+  int nelec;
+  double core_energy;
+  const double *h1;
+  const double *eri_packed;
+  size_t n_eri_packed;
+} sbd_tpb_hamiltonian;
+
+/* Results; pointer fields are caller-allocated (host) and may be NULL to skip that output. */
+typedef struct sbd_tpb_result {
+  double energy;      /* <W|H|W> with an FP64 sigma (tpb/sbdiag.h:431-469) */
+  double residual;    /* last Davidson residual norm */
+  int iterations;     /* Davidson steps (sigma applications inside the loop) */
+  int converged;      /* residual < eps */
+  double *ci_vector;  /* [na*nb] reference sign convention, index Ia*nb+Ib */
+  double *density;    /* [2L]: alpha/beta occupation per orbital, density[2p+s] */
+  double *one_rdm;    /* [2*L*L]  onebody[s][i + L*j] (tpb/correlation.h:378-664) */
+  double *two_rdm;    /* [4*L^4]  twobody[s+2t][...] in the reference layout */
+  double seconds_tables, seconds_davidson, seconds_rdm, seconds_total;
+} sbd_tpb_result;
+
+/* ---- one-shot driver: replaces sbd::tpb::diag (tpb/sbdiag.h:139-151, one rank, --method 0) */
+SBD_TPB_API int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
+                 const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                 sbd_tpb_result *result);
+
+/* ---- handle API: the stages of the same path, for callers that drive them ---------------- */
+SBD_TPB_API const char *sbd_tpb_last_error(void);
+SBD_TPB_API int sbd_tpb_create(int device, sbd_tpb_handle **out);
+SBD_TPB_API int sbd_tpb_destroy(sbd_tpb_handle *h);
+
+/* Replaces SetupIntegrals (basic/makeintegrals.h:123-174) feeding MultTPBThrust::Init
+ * (tpb/mult_thrust.h:98-277). */
+SBD_TPB_API int sbd_tpb_set_hamiltonian(sbd_tpb_handle *h, const sbd_tpb_hamiltonian *ham);
+
+/* Strings as LoadAlphaDets + sort_bitarray leave them (basic/makedeterminants.h:160-186):
+ * ascending and unique, or in the order --shuffle leaves them (ShuffleDet,
+ * basic/determinants.h:622-628); the order fixes the determinant index.  Rejected when
+ * duplicated, wider than norb, or when their electron counts differ within a spin. */
+SBD_TPB_API int sbd_tpb_set_strings(sbd_tpb_handle *h, const uint64_t *astr, size_t na, const uint64_t *bstr,
+                        size_t nb);
+
+/* Excitation tables on the GPU; replaces MakeHelpers/RemakeHelpers with GenerateExcitation
+ * (tpb/helper.h:185-323, 710-854, 916-1226) for one rank. */
+SBD_TPB_API int sbd_tpb_build_tables(sbd_tpb_handle *h);
+SBD_TPB_API int sbd_tpb_table_size(sbd_tpb_handle *h, int kind, size_t *nrows, size_t *nnz);
+/* Copies one table to host buffers in the reference's flattened layout: off[nrows+1] CSR
+ * offsets, ket[nnz] ket string indices (ascending per bra, TaskHelpers::*FromAlpha),
+ * cran[2*nnz] or [4*nnz] CrAn labels (TaskHelpers::*CrAn). */
+SBD_TPB_API int sbd_tpb_get_table(sbd_tpb_handle *h, int kind, uint64_t *off, uint64_t *ket, int32_t *cran);
+
+/* H_ii for every determinant; replaces makeQChamDiagTerms (tpb/qcham.h:290-340,
+ * tpb/mult_thrust.h:1585-1664). */
+SBD_TPB_API int sbd_tpb_diagonal(sbd_tpb_handle *h, double *hii, int mem);
+
+/* sigma (+)= H*C; replaces MultBase<double>::run(hii, Wk, Wb) (basic/mult.h:94-102) as
+ * implemented by MultTPBThrust::run (tpb/mult_thrust.h:1172-1582) and sbd::mult
+ * (tpb/mult.h:625-881).  accumulate = 1 adds into sigma like the reference (Wb accumulates);
+ * accumulate = 0 overwrites.  C and sigma use the reference sign convention. */
+SBD_TPB_API int sbd_tpb_sigma(sbd_tpb_handle *h, const double *C, double *sigma, int accumulate, int mem);
+/* FP32 vectors (mixed-precision path), same semantics. */
+SBD_TPB_API int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigma, int accumulate, int mem);
+
+/* Davidson (tpb/davidson.h:667-930; basic/davidson_thrust.h:85-373) on the handle's problem,
+ * from W (host, [na*nb], reference convention; NULL = HF start).  Writes the energy etc. into
+ * result (ci_vector/density/RDM fields as in sbd_tpb_diag). */
+SBD_TPB_API int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params, const double *W0,
+                     sbd_tpb_result *result);
+
+/* 1/2-RDMs of W; replaces Correlation (tpb/correlation.h:378-664) and
+ * MultTPBThrust::correlation (tpb/correlation_thrust.h:504-731).  one: [2*L*L], two: [4*L^4]
+ * (two may be NULL for the 1-RDM only).  W in the reference convention. */
+SBD_TPB_API int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, int mem);
+
+/* Device stream of the handle (cudaStream_t as void*), for callers that order their own work. */
+SBD_TPB_API void *sbd_tpb_stream(sbd_tpb_handle *h);
+
+/* Timing of the last sigma call on the handle's stream (CUDA events), milliseconds. */
+SBD_TPB_API double sbd_tpb_last_sigma_ms(sbd_tpb_handle *h);
+
+/* Number of kernel launches the library has issued on this handle (for accounting). */
+SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBD_TPB_H */

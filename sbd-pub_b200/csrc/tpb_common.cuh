@@ -1,0 +1,190 @@
+// Internal declarations shared by the CUDA translation units of libsbdtpb.
+//
+// Sign convention inside the library.  The reference evaluates every matrix element on the
+// interleaved determinant (alpha orbital p -> spin-orbital 2p, beta p -> 2p+1;
+// basic/determinants.h:97-142), so same-spin signs depend on the other spin's string.  The
+// library works in the separated ordering (all alpha creators, then all beta), where
+// H_sep = D H_ref D with D = diag((-1)^phi(Ia,Ib)) and phi = #{(p in Ia, q in Ib) : q < p}.
+// In that ordering the alpha part of H acts on the alpha index only (up to the diagonal-in-beta
+// Coulomb term of alpha singles), which is what lets sigma run as row/column SpMM and as a
+// gather -> dense (pq|rs) contraction -> scatter.  Energies, RDMs and iteration counts are
+// invariant; vectors crossing the C ABI are multiplied by D on the way in and out.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sbd_tpb.h"
+
+namespace sbdtpb {
+
+// ---- error plumbing: every CUDA call goes through this and turns into a status ------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+#define TPB_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      int code_ = (e_ == cudaErrorMemoryAllocation) ? SBD_TPB_ERR_OOM : SBD_TPB_ERR_CUDA;   \
+      return ::sbdtpb::fail(code_, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    }                                                                                       \
+  } while (0)
+
+#define TPB_LAUNCHED(h)                                                                     \
+  do {                                                                                      \
+    (h)->launches++;                                                                        \
+    cudaError_t e_ = cudaGetLastError();                                                    \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::sbdtpb::fail(SBD_TPB_ERR_CUDA, std::string("kernel launch: ") +              \
+                                                  cudaGetErrorString(e_));                  \
+  } while (0)
+
+#define TPB_CHECK(expr)            \
+  do {                             \
+    int rc_ = (expr);              \
+    if (rc_ != SBD_TPB_OK) return rc_; \
+  } while (0)
+
+// ---- device bit helpers ---------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t open_mask(int lo, int hi) {
+  // bits strictly between lo and hi (0 <= lo < hi <= 63)
+  return ((1ull << hi) - 1ull) & ~((2ull << lo) - 1ull);
+}
+
+__device__ __forceinline__ int lowest_bit(uint64_t x) { return __ffsll((long long)x) - 1; }
+__device__ __forceinline__ int highest_bit(uint64_t x) { return 63 - __clzll((long long)x); }
+
+// Sign bit (0 or 1) of the interleaved -> separated reordering of determinant (a, b):
+// parity of #{(p in a, q in b): q < p} = popcount(b & P(a)), P(a)_q = parity of a's bits > q.
+__host__ __device__ __forceinline__ uint64_t above_parity_mask(uint64_t a) {
+  uint64_t s = a;
+  s ^= s >> 1;
+  s ^= s >> 2;
+  s ^= s >> 4;
+  s ^= s >> 8;
+  s ^= s >> 16;
+  s ^= s >> 32;  // bit q = xor of a's bits at positions >= q
+  return s >> 1;  // bit q = xor of a's bits at positions > q
+}
+
+// ---- device-resident tables -----------------------------------------------------------------
+// One spin's excitation table in CSR form.  lab packs the spatial orbitals of an entry:
+// singles (cr | an << 8), doubles (cr0 | cr1 << 8 | an0 << 16 | an1 << 24), cr < 64.
+struct ExTable {
+  uint32_t *off = nullptr;  // [n+1]
+  uint32_t *ket = nullptr;  // [nnz]
+  uint32_t *lab = nullptr;  // [nnz]
+  size_t nnz = 0;
+  uint32_t max_row = 0;     // longest bra row
+};
+
+// One spin's sigma program: per bra string, singles then doubles, with the separated-convention
+// element.  For singles, pairsgn = +-(an*L + cr + 1) marks the other-spin Coulomb term
+// sgn * sum_{k in other string} (an cr|kk); 0 for doubles.
+struct SigmaProg {
+  uint32_t *off = nullptr;
+  uint32_t *ket = nullptr;
+  double *val = nullptr;
+  float *valf = nullptr;
+  int32_t *pairsgn = nullptr;
+  size_t nnz = 0;
+  uint32_t max_row = 0;  // longest row
+};
+
+// Dense-path data for the alpha-beta term as gather -> (pq|rs) contraction -> scatter.
+struct ABDense {
+  bool enabled = false;
+  int npq = 0, nrs = 0;           // distinct alpha / beta single labels
+  int *pq_of_label = nullptr;     // [npq] pair index p*L+q per label (device)
+  int *rs_of_label = nullptr;     // [nrs]
+  int32_t *a_label = nullptr;     // [nnz alpha singles] label id per entry (sign in bit 31)
+  int32_t *b_label = nullptr;     // [nnz beta singles]
+  uint32_t *a_off = nullptr, *a_ket = nullptr;  // alpha singles CSR (bra -> ket)
+  uint32_t *b_off = nullptr, *b_ket = nullptr;  // beta singles CSR
+  double *V = nullptr;            // [nrs][npq] (pq|rs), FP64
+  uint16_t *Vhi = nullptr, *Vlo = nullptr;  // split BF16 of V, K-major for the tensor-core path
+};
+
+}  // namespace sbdtpb
+
+struct sbd_tpb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint64_t launches = 0;
+  float last_sigma_ms = 0.f;
+  int num_sms = 148;
+  size_t smem_optin = 0;
+
+  // problem (host copies)
+  int L = 0, nelec = 0;
+  double I0 = 0.0;
+  std::vector<double> h1;          // L*L
+  std::vector<double> eri_packed;  // packed store
+  std::vector<uint64_t> astr, bstr;
+  int n_alpha = 0, n_beta = 0;
+  bool have_ham = false, have_strings = false, have_tables = false;
+
+  // device data
+  double *d_eri = nullptr;   // [L*L][L*L] full (pq|rs)
+  double *d_vd = nullptr;    // [L*L][L] (pq|kk)
+  double *d_J = nullptr;     // [L][L] (pp|qq)
+  uint64_t *d_astr = nullptr, *d_bstr = nullptr;
+  uint64_t *d_apar = nullptr;  // [na] above_parity_mask(astr)
+  double *d_Ea = nullptr, *d_Eb = nullptr;  // same-spin string energies
+  double *d_uJ = nullptr;    // [na][L]: sum_{p in Ia} (pp|qq)
+  double *d_hii = nullptr;   // [na*nb] FP64 diagonal
+  sbdtpb::ExTable ta_s, ta_d, tb_s, tb_d;
+  sbdtpb::SigmaProg pa, pb;
+  sbdtpb::ABDense ab;
+
+  // scratch
+  double *d_partials = nullptr;  // reduction partial sums
+  size_t partials_cap = 0;
+  double *d_tmp64 = nullptr;     // one N-vector FP64 (sign conversion staging)
+  double *d_tmp64b = nullptr;
+  float *d_tmp32 = nullptr, *d_tmp32b = nullptr;
+  void *d_ab_work = nullptr;     // dense alpha-beta intermediates
+  size_t ab_work_bytes = 0;
+  size_t ndet() const { return astr.size() * bstr.size(); }
+};
+
+namespace sbdtpb {
+// tables.cu
+int build_excitation_tables(sbd_tpb_handle *h);
+int copy_table_reference_layout(sbd_tpb_handle *h, int kind, uint64_t *off, uint64_t *ket,
+                                int32_t *cran);
+// hamiltonian.cu
+int upload_hamiltonian(sbd_tpb_handle *h);
+int build_string_data(sbd_tpb_handle *h);
+int build_sigma_programs(sbd_tpb_handle *h);
+int compute_diagonal(sbd_tpb_handle *h);
+void free_device_problem(sbd_tpb_handle *h);
+// sigma.cu
+template <typename T>
+int sigma_sep(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate);
+// sigma (+)= (H - shift) C
+template <typename T>
+int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, double shift);
+int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y);
+int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y);
+// ab_dense.cu: alpha-beta term as gather -> dense (pq|rs) contraction -> scatter
+int ab_dense_setup(sbd_tpb_handle *h, int enable);
+template <typename T>
+int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma);
+// vecops.cu
+int ensure_partials(sbd_tpb_handle *h, size_t n);
+template <typename T>
+int multi_dot(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n, double *out);
+// rdm.cu
+// W: device FP64 vector in the separated convention; outputs are host arrays (any may be null):
+// one [2L^2], two [4L^4] in the reference layouts, density [2L].
+int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double *density);
+// davidson.cu
+int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
+                 sbd_tpb_result *res);
+}  // namespace sbdtpb

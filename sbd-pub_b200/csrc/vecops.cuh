@@ -1,0 +1,46 @@
+// Davidson vector-kernel interfaces (see vecops.cu).
+#pragma once
+
+#include "tpb_common.cuh"
+
+namespace sbdtpb {
+
+constexpr int kVecThreads = 256;
+constexpr int kMaxSub = 16;            // largest Davidson subspace handled by the fused kernels
+constexpr int kMaxVec = kMaxSub + 2;   // values reduced per pass
+
+template <typename T>
+struct VecPtrs {
+  const T *p[kMaxVec];
+};
+
+struct CoefArray {
+  double v[kMaxSub];
+};
+
+template <typename T>
+struct ResidualArgs {
+  VecPtrs<T> C, HC;
+  double u[kMaxSub];  // lowest Ritz vector in the subspace basis
+  int m;              // subspace size
+  double e_shifted;   // Ritz value of (H - shift)
+  double e0;          // Ritz value of H
+  const double *hii;  // FP64 diagonal
+  T *W;               // Ritz vector out (may be null)
+  T *t;               // preconditioned correction out
+};
+
+int vec_blocks(sbd_tpb_handle *h);
+template <typename T>
+int residual_step(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, double *out);
+template <typename T>
+int cgs_update(sbd_tpb_handle *h, const T *const *C, int m, const double *o, T *t, size_t n,
+               int want_dots, double *out);
+template <typename T>
+int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n);
+template <typename S, typename D>
+int convert_vec(sbd_tpb_handle *h, const S *x, D *y, size_t n);
+template <typename T>
+int axpby(sbd_tpb_handle *h, const T *x, T *y, double a, double b, size_t n);
+
+}  // namespace sbdtpb

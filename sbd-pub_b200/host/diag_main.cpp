@@ -1,0 +1,154 @@
+// Drop-in `diag` CLI for the one-rank TPB selected-basis diagonalization on one B200.
+//
+// Mirrors apps/chemistry_tpb_selected_basis_diagonalization/main.cc and the flag parser of
+// tpb/sbdiag.h:52-122: same flags, same stdout lines (" Davidson iteration", " Energy = ",
+// " Sample-based diagonalization: ..."), same 1pRDM.txt / 2pRDM.txt files and energy
+// decomposition (main.cc:196-319).  Extra flags select the arithmetic and the correction:
+//   --precision fp64|mixed   --preconditioner diagonal|learned   --device N
+// Flags for parts outside this build (--loadname/--savename, carry-over selection,
+// --dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "sbd_tpb.h"
+#include "tpb_io.h"
+
+namespace {
+
+[[noreturn]] void die(const std::string &msg) {
+  std::cerr << "diag: " << msg << std::endl;
+  std::exit(1);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  std::string adetfile = "alphadets.txt", bdetfile, fcidumpfile = "fcidump.txt";
+  sbd_tpb_params prm;
+  sbd_tpb_default_params(&prm);
+  prm.verbose = 1;
+  int do_shuffle = 0, method = 0, carryover_type = 0, comm_sizes = 1;
+  size_t bit_length = 20;
+  std::string unsupported;
+  for (int i = 1; i < argc; i++) {
+    const std::string a(argv[i]);
+    auto next = [&]() -> std::string {
+      if (i + 1 >= argc) die("missing value for " + a);
+      return std::string(argv[++i]);
+    };
+    if (a == "--adetfile") adetfile = next();
+    else if (a == "--bdetfile") bdetfile = next();
+    else if (a == "--fcidump") fcidumpfile = next();
+    else if (a == "--method") method = std::atoi(next().c_str());
+    else if (a == "--iteration") prm.max_it = std::atoi(next().c_str());
+    else if (a == "--block") prm.max_nb = std::atoi(next().c_str());
+    else if (a == "--tolerance") prm.eps = std::atof(next().c_str());
+    else if (a == "--max_time") prm.max_time = std::atof(next().c_str());
+    else if (a == "--init") prm.init = std::atoi(next().c_str());
+    else if (a == "--seed") next();
+    else if (a == "--shuffle") do_shuffle = std::atoi(next().c_str());
+    else if (a == "--rdm") prm.do_rdm = std::atoi(next().c_str());
+    else if (a == "--bit_length") bit_length = std::strtoul(next().c_str(), nullptr, 10);
+    else if (a == "--carryover_type") carryover_type = std::atoi(next().c_str());
+    else if (a == "--carryover_ratio" || a == "--carryover_threshold" ||
+             a == "--carryover_adetfile" || a == "--carryover_bdetfile") next();
+    else if (a == "--adet_comm_size" || a == "--bdet_comm_size" || a == "--task_comm_size")
+      comm_sizes *= std::atoi(next().c_str());
+    else if (a == "--loadname" || a == "--savename" || a == "--dump_matrix_form_wf") {
+      const std::string v = next();
+      if (!v.empty()) unsupported += " " + a;
+    } else if (a == "--precision") {
+      const std::string v = next();
+      if (v == "fp64") prm.precision = SBD_TPB_FP64;
+      else if (v == "mixed") prm.precision = SBD_TPB_MIXED;
+      else die("--precision must be fp64 or mixed");
+    } else if (a == "--preconditioner") {
+      const std::string v = next();
+      if (v == "diagonal") prm.preconditioner = SBD_TPB_PRECOND_DIAGONAL;
+      else if (v == "learned") prm.preconditioner = SBD_TPB_PRECOND_LEARNED;
+      else die("--preconditioner must be diagonal or learned");
+    } else if (a == "--device") prm.device = std::atoi(next().c_str());
+    else if (a == "--use_precalculated_dets" || a == "--max_memory_gb_for_determinants" ||
+             a == "--thrust_collapse_loops") next();
+  }
+  (void)bit_length;
+  if (method != 0) die("only --method 0 (matrix-free Davidson) is built");
+  if (comm_sizes != 1) die("one rank on one GPU: --*_comm_size must be 1");
+  if (prm.init != 0) die("only --init 0 (start from the first determinant) is built");
+  if (carryover_type != 0) die("carry-over string selection is not built (--carryover_type 0)");
+  if (!unsupported.empty()) die("not built in this version:" + unsupported);
+
+  std::cout.precision(16);
+  tpbio::FciDump fd;
+  std::string err;
+  if (!tpbio::load_fcidump(fcidumpfile, fd, &err)) die(err);
+  const int L = fd.norb;
+  std::vector<uint64_t> adet, bdet;
+  if (!tpbio::load_strings(adetfile, L, adet, &err)) die(err);
+  if (bdetfile.empty()) bdet = adet;
+  else if (!tpbio::load_strings(bdetfile, L, bdet, &err)) die(err);
+  if (do_shuffle) {
+    tpbio::shuffle_strings(adet, 1729);
+    tpbio::shuffle_strings(bdet, 137);
+  }
+  const size_t na = adet.size(), nb = bdet.size();
+  std::vector<double> W(na * nb), density(2 * L);
+  std::vector<double> one, two;
+  if (prm.do_rdm) {
+    one.resize(2 * (size_t)L * L);
+    two.resize(4 * (size_t)L * L * L * L);
+  }
+  sbd_tpb_hamiltonian ham{L, fd.nelec, fd.core, fd.h1.data(), fd.eri_packed.data(), fd.eri_packed.size()};
+  sbd_tpb_result res;
+  std::memset(&res, 0, sizeof(res));
+  res.ci_vector = W.data();
+  res.density = density.data();
+  res.one_rdm = prm.do_rdm ? one.data() : nullptr;
+  res.two_rdm = prm.do_rdm ? two.data() : nullptr;
+  const int rc = sbd_tpb_diag(&prm, &ham, adet.data(), na, bdet.data(), nb, &res);
+  if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(sbd_tpb_last_error());
+  std::cout << " Elapsed time for helper construction " << res.seconds_tables << " (sec) " << std::endl;
+  std::cout << " Elapsed time for davidson " << res.seconds_davidson << " (sec) " << std::endl;
+  std::cout << " Energy = " << res.energy << std::endl;
+  std::cout << " Sample-based diagonalization: Energy = " << res.energy << std::endl;
+  std::cout << " Sample-based diagonalization: density = ";
+  for (int i = 0; i < L; i++) std::cout << ((i == 0) ? "[" : ",") << density[2 * i] + density[2 * i + 1];
+  std::cout << std::endl;
+  std::cout << " Sample-based diagonalization: carryover bitstrings = [], size = 0" << std::endl;
+  if (prm.do_rdm) {
+    // 1pRDM.txt / 2pRDM.txt and the energy decomposition (main.cc:264-317)
+    const size_t L2 = (size_t)L * L, L4 = L2 * L2;
+    double onebody = 0.0, twobody = 0.0;
+    std::ofstream o1("1pRDM.txt");
+    o1.precision(16);
+    for (int io = 0; io < L; io++)
+      for (int jo = 0; jo < L; jo++) {
+        const double g = one[io + (size_t)L * jo] + one[L2 + io + (size_t)L * jo];
+        o1 << io << " " << jo << " " << g << std::endl;
+        onebody += fd.h1[(size_t)io * L + jo] * g;
+      }
+    std::ofstream o2("2pRDM.txt");
+    o2.precision(16);
+    for (int io = 0; io < L; io++)
+      for (int jo = 0; jo < L; jo++)
+        for (int ia = 0; ia < L; ia++)
+          for (int ja = 0; ja < L; ja++) {
+            const size_t k = io + (size_t)L * jo + L2 * (ia + (size_t)L * ja);
+            const double G = two[k] + two[L4 + k] + two[2 * L4 + k] + two[3 * L4 + k];
+            o2 << io << " " << jo << " " << ia << " " << ja << " " << G << std::endl;
+            twobody += 0.5 * fd.eri_packed[tpbio::packed_index(io, ia, jo, ja)] * G;
+          }
+    std::cout << " Zero-Body energy = " << fd.core << std::endl;
+    std::cout << " One-Body energy = " << onebody << std::endl;
+    std::cout << " Two-Body energy = " << twobody << std::endl;
+    std::cout << " One-Body + Two-Body energy = " << onebody + twobody << std::endl;
+    std::cout << " Zero-Body + One-Body + Two-Body energy = " << fd.core + onebody + twobody << std::endl;
+  }
+  return 0;
+}

@@ -1,0 +1,36 @@
+// Host-side input parsing for the drop-in `diag` CLI: FCIDUMP and alpha/beta string files.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tpbio {
+
+struct FciDump {
+  int norb = 0;
+  int nelec = 0;
+  int ms2 = 0;
+  double core = 0.0;
+  std::vector<double> h1;          // norb*norb, row-major, symmetric
+  std::vector<double> eri_packed;  // 8-fold packed store (basic/integrals.h:64-107)
+};
+
+// FCIDUMP text as framework/fcidump.h:29-141 reads it and basic/makeintegrals.h:123-174 stores
+// it.  Returns false with *err set on failure.
+bool load_fcidump(const std::string &path, FciDump &out, std::string *err);
+
+// One string per line, orbital 0 is the last character (framework/bit_manipulation.h:215-230);
+// sorted ascending and duplicates removed (sort_bitarray, bit_manipulation.h:381-392).
+bool load_strings(const std::string &path, int norb, std::vector<uint64_t> &out, std::string *err);
+
+// Text form of a string as sbd::makestring prints it (orbital norb-1 first).
+std::string make_string(uint64_t s, int norb);
+
+// Reference's ShuffleDet (basic/determinants.h:622-628): keep entry 0, shuffle the rest with
+// std::mt19937(seed).
+void shuffle_strings(std::vector<uint64_t> &s, unsigned int seed);
+
+size_t packed_index(int i, int j, int k, int l);
+
+}  // namespace tpbio

@@ -1,0 +1,287 @@
+"""ctypes binding of libsbdtpb (the C ABI in include/sbd_tpb.h).
+
+Python-side mirror of the reference's one-rank TPB entry points: ``diag`` replaces
+``sbd::tpb::diag`` (tpb/sbdiag.h:139-151) and ``Handle`` exposes the stages it is made of --
+excitation tables (tpb/helper.h:185-323), the diagonal (tpb/qcham.h:290-340), sigma
+(``MultBase::run``, basic/mult.h:94-102), Davidson (tpb/davidson.h:667-930) and the RDMs
+(tpb/correlation.h:378-664).  Every call goes to the CUDA library; there is no CPU fallback:
+loading raises when ``lib/libsbdtpb.so`` is missing and calls raise ``TpbError`` with the
+library's message on any failure status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libsbdtpb.so")
+
+OK = 0
+ERR_INVALID = -1
+ERR_CUDA = -2
+ERR_OOM = -3
+ERR_NOT_CONVERGED = -4
+ERR_STATE = -5
+ERR_IO = -6
+ERR_NO_DEVICE = -7
+HOST, DEVICE = 0, 1
+SINGLES_ALPHA, DOUBLES_ALPHA, SINGLES_BETA, DOUBLES_BETA = 0, 1, 2, 3
+FP64, MIXED = 0, 1
+PRECOND_DIAGONAL, PRECOND_LEARNED = 0, 1
+
+# Every function the header declares (the symbol test checks the library against this list).
+EXPORTED = [
+    "sbd_tpb_default_params", "sbd_tpb_diag", "sbd_tpb_last_error", "sbd_tpb_create",
+    "sbd_tpb_destroy", "sbd_tpb_set_hamiltonian", "sbd_tpb_set_strings", "sbd_tpb_build_tables",
+    "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
+    "sbd_tpb_sigma_f32", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
+    "sbd_tpb_last_sigma_ms", "sbd_tpb_kernel_launches",
+]
+
+
+class TpbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"sbd_tpb error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("max_it", C.c_int), ("max_nb", C.c_int), ("eps", C.c_double), ("max_time", C.c_double),
+        ("init", C.c_int), ("do_rdm", C.c_int), ("precision", C.c_int), ("preconditioner", C.c_int),
+        ("verbose", C.c_int), ("device", C.c_int),
+    ]
+
+
+class Hamiltonian(C.Structure):
+    _fields_ = [
+        ("norb", C.c_int), ("nelec", C.c_int), ("core_energy", C.c_double),
+        ("h1", C.POINTER(C.c_double)), ("eri_packed", C.POINTER(C.c_double)),
+        ("n_eri_packed", C.c_size_t),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("energy", C.c_double), ("residual", C.c_double), ("iterations", C.c_int),
+        ("converged", C.c_int), ("ci_vector", C.POINTER(C.c_double)),
+        ("density", C.POINTER(C.c_double)), ("one_rdm", C.POINTER(C.c_double)),
+        ("two_rdm", C.POINTER(C.c_double)), ("seconds_tables", C.c_double),
+        ("seconds_davidson", C.c_double), ("seconds_rdm", C.c_double),
+        ("seconds_total", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libsbdtpb.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C sbd-pub_b200`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.sbd_tpb_last_error.restype = C.c_char_p
+    L.sbd_tpb_default_params.argtypes = [C.POINTER(Params)]
+    L.sbd_tpb_diag.argtypes = [C.POINTER(Params), C.POINTER(Hamiltonian), vp, C.c_size_t, vp,
+                               C.c_size_t, C.POINTER(Result)]
+    L.sbd_tpb_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.sbd_tpb_destroy.argtypes = [vp]
+    L.sbd_tpb_set_hamiltonian.argtypes = [vp, C.POINTER(Hamiltonian)]
+    L.sbd_tpb_set_strings.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t]
+    L.sbd_tpb_build_tables.argtypes = [vp]
+    L.sbd_tpb_table_size.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    L.sbd_tpb_get_table.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.sbd_tpb_diagonal.argtypes = [vp, vp, C.c_int]
+    L.sbd_tpb_sigma.argtypes = [vp, vp, vp, C.c_int, C.c_int]
+    L.sbd_tpb_sigma_f32.argtypes = [vp, vp, vp, C.c_int, C.c_int]
+    L.sbd_tpb_davidson.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
+    L.sbd_tpb_rdm.argtypes = [vp, vp, vp, vp, C.c_int]
+    L.sbd_tpb_stream.restype = vp
+    L.sbd_tpb_stream.argtypes = [vp]
+    L.sbd_tpb_last_sigma_ms.restype = C.c_double
+    L.sbd_tpb_last_sigma_ms.argtypes = [vp]
+    L.sbd_tpb_kernel_launches.restype = C.c_uint64
+    L.sbd_tpb_kernel_launches.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _check(rc: int, allow=(OK,)):
+    if rc not in allow:
+        raise TpbError(rc, lib().sbd_tpb_last_error().decode(errors="replace"))
+    return rc
+
+
+def _ptr(a) -> int:
+    """Address of a C-contiguous numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor (host or device)
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().sbd_tpb_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+@dataclass
+class Problem:
+    """An FCIDUMP-style Hamiltonian and its alpha/beta strings (host numpy arrays)."""
+    norb: int
+    nelec: int
+    core: float
+    h1: np.ndarray          # [L, L] float64
+    eri_packed: np.ndarray  # packed 8-fold store, float64
+    astr: np.ndarray        # uint64
+    bstr: np.ndarray        # uint64
+
+    def ham_struct(self) -> Hamiltonian:
+        self._h1c = np.ascontiguousarray(self.h1, np.float64)
+        self._eric = np.ascontiguousarray(self.eri_packed, np.float64)
+        return Hamiltonian(self.norb, self.nelec, self.core,
+                           self._h1c.ctypes.data_as(C.POINTER(C.c_double)),
+                           self._eric.ctypes.data_as(C.POINTER(C.c_double)), self._eric.size)
+
+    @property
+    def ndet(self) -> int:
+        return len(self.astr) * len(self.bstr)
+
+
+class Handle:
+    """One GPU, one problem: tables, diagonal, sigma, Davidson and RDMs (include/sbd_tpb.h)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        _check(lib().sbd_tpb_create(device, C.byref(self.h)))
+        self.problem: Problem | None = None
+
+    def close(self):
+        if self.h:
+            lib().sbd_tpb_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_problem(self, prob: Problem, build: bool = True):
+        self.problem = prob
+        hs = prob.ham_struct()
+        _check(lib().sbd_tpb_set_hamiltonian(self.h, C.byref(hs)))
+        a = np.ascontiguousarray(prob.astr, np.uint64)
+        b = np.ascontiguousarray(prob.bstr, np.uint64)
+        _check(lib().sbd_tpb_set_strings(self.h, a.ctypes.data, len(a), b.ctypes.data, len(b)))
+        if build:
+            self.build_tables()
+
+    def build_tables(self):
+        _check(lib().sbd_tpb_build_tables(self.h))
+
+    def table(self, kind: int):
+        """(off[n+1] u64, ket[nnz] u64, cran[2|4 * nnz] i32) in the reference layout."""
+        nrows, nnz = C.c_size_t(), C.c_size_t()
+        _check(lib().sbd_tpb_table_size(self.h, kind, C.byref(nrows), C.byref(nnz)))
+        per = 2 if kind in (SINGLES_ALPHA, SINGLES_BETA) else 4
+        off = np.zeros(nrows.value + 1, np.uint64)
+        ket = np.zeros(max(nnz.value, 1), np.uint64)
+        cran = np.zeros(max(nnz.value, 1) * per, np.int32)
+        _check(lib().sbd_tpb_get_table(self.h, kind, off.ctypes.data, ket.ctypes.data, cran.ctypes.data))
+        return off, ket[: nnz.value], cran[: nnz.value * per]
+
+    def diagonal(self) -> np.ndarray:
+        out = np.zeros(self.problem.ndet)
+        _check(lib().sbd_tpb_diagonal(self.h, out.ctypes.data, HOST))
+        return out
+
+    def sigma(self, C_, out=None, accumulate: bool = False):
+        """sigma (+)= H C for numpy (host) or torch CUDA (device) vectors, float64 or float32."""
+        dev = not isinstance(C_, np.ndarray)
+        if out is None:
+            if dev:
+                import torch
+                out = torch.zeros_like(C_)
+            else:
+                out = np.zeros_like(C_)
+        f32 = (C_.dtype == np.float32) if not dev else (str(C_.dtype) == "torch.float32")
+        fn = lib().sbd_tpb_sigma_f32 if f32 else lib().sbd_tpb_sigma
+        _check(fn(self.h, _ptr(C_), _ptr(out), int(accumulate), DEVICE if dev else HOST))
+        return out
+
+    def last_sigma_ms(self) -> float:
+        return lib().sbd_tpb_last_sigma_ms(self.h)
+
+    def kernel_launches(self) -> int:
+        return int(lib().sbd_tpb_kernel_launches(self.h))
+
+    def stream(self) -> int:
+        return lib().sbd_tpb_stream(self.h) or 0
+
+    def davidson(self, params: Params | None = None, W0: np.ndarray | None = None,
+                 want_vector=True, want_rdm=False):
+        prob = self.problem
+        params = params or default_params()
+        res = Result()
+        W = np.zeros(prob.ndet) if want_vector else None
+        dens = np.zeros(2 * prob.norb)
+        one = np.zeros(2 * prob.norb ** 2) if want_rdm else None
+        two = np.zeros(4 * prob.norb ** 4) if want_rdm else None
+        dp = C.POINTER(C.c_double)
+        res.ci_vector = W.ctypes.data_as(dp) if W is not None else dp()
+        res.density = dens.ctypes.data_as(dp)
+        res.one_rdm = one.ctypes.data_as(dp) if one is not None else dp()
+        res.two_rdm = two.ctypes.data_as(dp) if two is not None else dp()
+        w0 = None if W0 is None else np.ascontiguousarray(W0, np.float64)
+        rc = lib().sbd_tpb_davidson(self.h, C.byref(params), w0.ctypes.data if w0 is not None else None,
+                                    C.byref(res))
+        _check(rc, allow=(OK, ERR_NOT_CONVERGED))
+        return dict(energy=res.energy, residual=res.residual, iterations=res.iterations,
+                    converged=bool(res.converged), W=W, density=dens, one=one, two=two,
+                    seconds=res.seconds_davidson)
+
+    def rdm(self, W: np.ndarray, two_body=True):
+        L = self.problem.norb
+        one = np.zeros(2 * L * L)
+        two = np.zeros(4 * L ** 4) if two_body else None
+        w = np.ascontiguousarray(W, np.float64)
+        _check(lib().sbd_tpb_rdm(self.h, w.ctypes.data, one.ctypes.data,
+                                 two.ctypes.data if two is not None else None, HOST))
+        return one, two
+
+
+def diag(prob: Problem, params: Params | None = None, want_rdm=False):
+    """One-shot solve: sbd::tpb::diag for one rank (tpb/sbdiag.h:139-151)."""
+    params = params or default_params()
+    res = Result()
+    W = np.zeros(prob.ndet)
+    dens = np.zeros(2 * prob.norb)
+    one = np.zeros(2 * prob.norb ** 2) if want_rdm else None
+    two = np.zeros(4 * prob.norb ** 4) if want_rdm else None
+    dp = C.POINTER(C.c_double)
+    res.ci_vector = W.ctypes.data_as(dp)
+    res.density = dens.ctypes.data_as(dp)
+    res.one_rdm = one.ctypes.data_as(dp) if one is not None else dp()
+    res.two_rdm = two.ctypes.data_as(dp) if two is not None else dp()
+    params.do_rdm = int(want_rdm)
+    hs = prob.ham_struct()
+    a = np.ascontiguousarray(prob.astr, np.uint64)
+    b = np.ascontiguousarray(prob.bstr, np.uint64)
+    rc = lib().sbd_tpb_diag(C.byref(params), C.byref(hs), a.ctypes.data, len(a), b.ctypes.data,
+                            len(b), C.byref(res))
+    _check(rc, allow=(OK, ERR_NOT_CONVERGED))
+    return dict(energy=res.energy, residual=res.residual, iterations=res.iterations,
+                converged=bool(res.converged), W=W, density=dens, one=one, two=two,
+                seconds_tables=res.seconds_tables, seconds_davidson=res.seconds_davidson,
+                seconds_total=res.seconds_total)

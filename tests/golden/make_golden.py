@@ -1,0 +1,145 @@
+"""Generate the golden fixtures of this directory from the reference itself.
+
+Runs the reference's own TPB code (compiled unchanged by ``make -C oracle ref`` into
+oracle/_ref/ref_dump, single-rank MPI shim) on small inputs and stores what it produced:
+excitation tables, the diagonal, one sigma of a seeded vector, the Davidson energy/vector and
+the RDMs.  Large arrays are stored whole when small and as sampled entries plus checksums
+otherwise, so the fixtures stay a few MB.  Needs the reference checkout (REF, default
+/root/reference); the committed .npz files are what the tests read.
+
+    python tests/golden/make_golden.py [case ...]
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "sbd-pub_b200", "python"))
+import synth  # noqa: E402
+
+REF = os.environ.get("REF", "/root/reference")
+DUMP = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+
+
+def _synthetic_inputs(tmp, L, na_e, nb_e, na_cnt, nb_cnt, seed):
+    h1, eri, core = synth.synthetic_hamiltonian(L, seed)
+    fd = os.path.join(tmp, "fcidump.txt")
+    synth.write_fcidump(fd, L, na_e + nb_e, h1, eri, core, ms2=na_e - nb_e)
+    a = synth.sample_strings(L, na_e, na_cnt, seed=seed + 1)
+    b = synth.sample_strings(L, nb_e, nb_cnt, seed=seed + 2)
+    fa, fb = os.path.join(tmp, "a.txt"), os.path.join(tmp, "b.txt")
+    synth.write_strings(fa, a, L)
+    synth.write_strings(fb, b, L)
+    return fd, fa, fb
+
+
+CASES = {
+    # name: (inputs, davidson (it, nb, tol), rdm, store_full)
+    "n2_1em3": dict(fcidump=f"{REF}/data/n2/fcidump.txt", adet=f"{REF}/data/n2/1em3-alpha.txt",
+                    davidson=(10, 10, 1e-8), rdm=True, full=False,
+                    published=-109.04162110, published_src="data/n2/README.md:5"),
+    "h2o_1em3": dict(fcidump=f"{REF}/data/h2o/fcidump.txt", adet=f"{REF}/data/h2o/h2o-1em3-alpha.txt",
+                     davidson=(10, 10, 1e-8), rdm=False, full=False,
+                     published=-76.23594663, published_src="data/h2o/README.md:6"),
+    "syn8": dict(synthetic=(8, 3, 3, 56, 56, 11), davidson=(10, 10, 1e-10), rdm=True, full=True),
+    "syn10_ab": dict(synthetic=(10, 4, 3, 120, 90, 23), davidson=(10, 10, 1e-10), rdm=True, full=True),
+    "fci12": dict(synthetic_named="fci12", davidson=(10, 10, 1e-8), rdm=False, full=False),
+}
+
+
+def run_case(name: str, spec: dict, out_dir: str):
+    with tempfile.TemporaryDirectory() as tmp:
+        bdet = None
+        if "synthetic" in spec:
+            fd, fa, fb = _synthetic_inputs(tmp, *spec["synthetic"])
+            bdet = fb
+        elif "synthetic_named" in spec:
+            L, n, cnt = synth.CONFIGS[spec["synthetic_named"]]
+            h1, eri, core = synth.synthetic_hamiltonian(L)
+            fd = os.path.join(tmp, "fcidump.txt")
+            fa = os.path.join(tmp, "a.txt")
+            synth.write_fcidump(fd, L, 2 * n, h1, eri, core)
+            synth.write_strings(fa, synth.sample_strings(L, n, cnt), L)
+        else:
+            fd, fa = spec["fcidump"], spec["adet"]
+        cmd = [DUMP, "--fcidump", fd, "--adetfile", fa, "--out", tmp, "--sigma_seed", "7"]
+        if bdet:
+            cmd += ["--bdetfile", bdet]
+        it, nb, tol = spec["davidson"]
+        cmd += ["--davidson", str(it), str(nb), repr(tol)]
+        if spec["rdm"]:
+            cmd += ["--rdm"]
+        env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+        subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+        L = synth.read_fcidump(fd)[0]
+        rd = lambda f, dt=np.float64: np.fromfile(os.path.join(tmp, f), dtype=dt)  # noqa: E731
+        astr, bstr = rd("astr.u64", np.uint64), rd("bstr.u64", np.uint64)
+        n = len(astr) * len(bstr)
+        rng = np.random.default_rng(0)
+        idx = np.unique(rng.integers(0, n, size=min(n, 512)))
+        data = dict(astr=astr, bstr=bstr, idx=idx)
+        tasks = [list(map(int, l.split())) for l in open(os.path.join(tmp, "tasks.txt"))]
+        data["tasks"] = np.array(tasks, dtype=np.int64)
+        # task 0 = type 2 (alpha singles, doubles); task 1 = type 1 (beta); task 2 = type 0
+        for t, kinds in ((0, ("sa", "da")), (1, ("sb", "db")), (2, ("sa", "sb"))):
+            for k in kinds:
+                off = rd(f"task{t}_{k}_off.u64", np.uint64)
+                ket = rd(f"task{t}_{k}_ket.u64", np.uint64).astype(np.uint32)
+                cran = rd(f"task{t}_{k}_cran.i32", np.int32).astype(np.int8)
+                data[f"t{t}_{k}_off"] = off
+                data[f"t{t}_{k}_ket"] = ket
+                data[f"t{t}_{k}_cran"] = cran
+        for vec in ("hii", "sigma_in", "sigma_out", "W"):
+            v = rd(f"{vec}.f64")
+            if spec["full"]:
+                data[vec] = v
+            data[vec + "_sample"] = v[idx]
+            data[vec + "_sum"] = np.array([v.sum(), (v * v).sum(), np.abs(v).sum()])
+        data["energy"] = np.array([float(open(os.path.join(tmp, "davidson.txt")).read())])
+        if spec["rdm"]:
+            r1, r2 = rd("rdm1.f64"), rd("rdm2.f64")
+            data["rdm1"] = r1
+            if spec["full"]:
+                data["rdm2"] = r2
+            ridx = np.unique(rng.integers(0, len(r2), size=min(len(r2), 4096)))
+            data["rdm2_idx"] = ridx
+            data["rdm2_sample"] = r2[ridx]
+            data["rdm2_sum"] = np.array([r2.sum(), (r2 * r2).sum(), np.abs(r2).sum()])
+        # the integrals as the reference's SetupIntegrals holds them (h1, packed store, core)
+        _, _, h1, eri, core = synth.read_fcidump(fd)
+        data["h1"], data["eri"], data["core"] = h1, eri, np.array([core])
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **data)
+        meta = dict(norb=L, na=len(astr), nb=len(bstr), energy=float(data["energy"][0]),
+                    davidson=list(spec["davidson"]), rdm=spec["rdm"], full=spec["full"])
+        for k in ("published", "published_src"):
+            if k in spec:
+                meta[k] = spec[k]
+        if "fcidump" in spec:
+            meta["fcidump"] = os.path.relpath(spec["fcidump"], REF)
+            meta["adet"] = os.path.relpath(spec["adet"], REF)
+        if "synthetic" in spec:
+            meta["synthetic"] = list(spec["synthetic"])
+        if "synthetic_named" in spec:
+            meta["synthetic_named"] = spec["synthetic_named"]
+        return meta
+
+
+def main():
+    names = sys.argv[1:] or list(CASES)
+    index_path = os.path.join(HERE, "cases.json")
+    index = json.load(open(index_path)) if os.path.exists(index_path) else {}
+    for name in names:
+        print("case", name, flush=True)
+        index[name] = run_case(name, CASES[name], HERE)
+        json.dump(index, open(index_path, "w"), indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
