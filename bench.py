@@ -1,0 +1,342 @@
+"""Benchmark of the TPB sigma hot path on B200 (one JSON line on rank 0).
+
+A step is one sigma = H*C over the whole determinant space of the workload (default: norb=32,
+10+10 electrons, 20,000 x 20,000 strings = 400M determinants, seeded synthetic integrals and
+strings as the reference's molecular inputs would give them).  `value` is sigma GDets/s with the
+vectors resident in HBM (the library's internal sign convention, no conversion passes); `e2e`
+is the same through the reference-facing C ABI call sbd_tpb_sigma with host buffers (H2D of C,
+sign conversions, D2H of sigma inside the timed region).  Multi-GPU runs are replicas (the
+path has no data exchange on one node in this build): every rank solves its own copy and
+`value` is the aggregate.  `--impl reference` times the reference's own CPU sigma (compiled
+unchanged under oracle/_ref) on a bounded sample of the same workload with all host threads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload sci32]
+                    [--precision mixed|fp64] [--impl ours|reference] [--no-solve]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sbd-pub_b200", "python"))
+
+METRIC = "sigma GDets/s; time to 1e-6 Ha: mixed+learned vs plain FP64, 1 B200"
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="sci32")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution solves")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_reference_sigma(prob_name, seconds_target, reps=1, threads=None):
+    """Time the reference's CPU sigma (oracle/_ref/ref_bench) on the first `amax` alpha strings x
+    all beta strings of the workload; amax is sized so the sample takes ~seconds_target."""
+    import synth
+    if not os.path.exists(REF_BENCH):
+        return None
+    L, n, cnt = synth.CONFIGS[prob_name]
+    h1, eri, core = synth.synthetic_hamiltonian(L)
+    strs = synth.sample_strings(L, n, cnt)
+    env = dict(os.environ)
+    threads = threads or os.cpu_count()
+    env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as tmp:
+        fd, fa = os.path.join(tmp, "fcidump.txt"), os.path.join(tmp, "a.txt")
+        synth.write_fcidump(fd, L, 2 * n, h1, eri, core)
+        synth.write_strings(fa, strs, L)
+
+        def run(amax, reps_):
+            out = subprocess.run([REF_BENCH, "--fcidump", fd, "--adetfile", fa, "--amax", str(amax),
+                                  "--reps", str(reps_)], capture_output=True, text=True, env=env,
+                                 check=True).stdout
+            kv = dict(tok.split("=", 1) for tok in out.split())
+            return int(kv["ndet"]), [float(x) for x in kv["sigma_s"].split(",")], float(kv["helper_s"])
+
+        amax = max(2, min(len(strs), 16))
+        ndet, ts, _ = run(amax, 1)
+        per_det = max(ts[0], 1e-4) / ndet
+        amax = int(min(len(strs), max(2, seconds_target / per_det / len(strs))))
+        ndet, ts, helper_s = run(amax, reps)
+    return dict(ndet=ndet, amax=amax, sigma_s=ts, helper_s=helper_s, threads=threads,
+                nstrings=len(strs))
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import synth
+    L, n, cnt = synth.CONFIGS[args.workload]
+    if not os.path.exists(REF_BENCH):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built "
+                          "(needs the reference checkout at build time)"}))
+        return
+    per_step = max(1.0, args.cpu_sample_seconds / max(1, args.steps))
+    r = cpu_reference_sigma(args.workload, per_step, reps=args.warmup + args.steps)
+    ts = r["sigma_s"][args.warmup:]
+    t = sum(ts)
+    val = r["ndet"] * len(ts) / t / 1e9
+    sample = (f"first {r['amax']} of {r['nstrings']} alpha strings x all {r['nstrings']} beta "
+              f"strings ({r['ndet']} determinants) per step, reference sbd::mult (tpb/mult.h:625-881)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "GDets/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(ts),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"{args.workload}: norb={L}, {n}+{n} electrons, "
+                                        f"{cnt} x {cnt} strings", "sample": sample},
+        "cpu_baseline": {"value": val, "unit": "GDets/s", "cores": r["threads"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": val, "unit": "GDets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def end_to_end(h, x, N, dt, esz, world):
+    import torch
+    xh = torch.empty(N, dtype=dt, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(N, dtype=dt, pin_memory=True)
+    xn, yn = xh.numpy(), yh.numpy()
+    h.sigma(xn, yn)
+    torch.cuda.synchronize()
+    steps = 5
+    te = time.perf_counter()
+    for _ in range(steps):
+        h.sigma(xn, yn)
+    e2e_s = (time.perf_counter() - te) / steps
+    return {"value": world * N / e2e_s / 1e9, "unit": "GDets/s", "h2d_bytes_per_step": N * esz,
+            "d2h_bytes_per_step": N * esz, "api": "sbd_tpb_sigma / sbd_tpb_sigma_f32 (host buffers)"}
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+
+    import sbd_tpb
+    import synth
+    torch.cuda.set_device(local)
+    L, n, cnt = synth.CONFIGS[args.workload]
+    prob = synth.make_problem(args.workload)
+    N = prob.ndet
+    h = sbd_tpb.Handle(local)
+    t0 = time.time()
+    h.set_problem(prob, build=False)
+    t1 = time.time()
+    h.build_tables()
+    t_tables = time.time() - t1
+    dt = torch.float32 if args.precision == "mixed" else torch.float64
+    esz = 4 if dt == torch.float32 else 8
+    gen = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
+    x = torch.randn(N, dtype=dt, device=f"cuda:{local}", generator=gen)
+    x /= torch.linalg.vector_norm(x)
+    y = torch.empty_like(x)
+    stream = torch.cuda.ExternalStream(h.stream(), device=f"cuda:{local}")
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        h.sigma_device(x, y)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = h.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            h.sigma_device(x, y)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = ev0.elapsed_time(ev1)
+    launches = h.kernel_launches() - launches0
+    barrier()
+    ms_max = ms_total
+    if pg is not None:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * N * args.steps / (ms_max * 1e-3) / 1e9
+
+    # per-kernel times of the same sigma (separate pass: reading them synchronises each call)
+    kern = []
+    for _ in range(max(3, min(args.steps, 10))):
+        h.sigma_device(x, y)
+        kern.append(h.last_sigma_kernels())
+    kern = np.array(kern).mean(axis=0)
+    pa_nnz = sum(int(h.table(k)[1].size) for k in (0, 1))
+    pb_nnz = sum(int(h.table(k)[1].size) for k in (2, 3))
+    val_b = esz  # sigma element values are stored at the vector precision
+    tab_row = pb_nnz * (4 + val_b + 4) + 4 * (len(prob.bstr) + 1)
+    tab_slab = pa_nnz * (4 + val_b + 4) + 4 * (len(prob.astr) + 1)
+    bytes_row = N * esz + N * esz + N * 8 + tab_row       # read C, write sigma, read H_ii, tables
+    bytes_slab = N * esz + 2 * N * esz + tab_slab         # read C, sigma read-modify-write, tables
+    names = ["sigma_row_kernel", "sigma_alpha_slab_kernel"]
+    per = [bytes_row, bytes_slab]
+    dom = int(np.argmax(kern))
+    pk = peaks()
+    achieved = per[dom] / (kern[dom] * 1e-3) / 1e9
+    roofline = {"kernel": names[dom], "bound": "hbm", "achieved": achieved,
+                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                "traffic": None, "peak_source": "measured" if not pk.get("fallback") else "fallback",
+                "kernel_ms": {names[i]: float(kern[i]) for i in range(len(kern))},
+                "algorithmic_bytes": {names[i]: int(per[i]) for i in range(len(kern))}}
+
+    # end to end through the reference-facing C ABI: host buffers, copies and sign passes timed
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(h, x, N, dt, esz, world)
+
+    solve = None
+    if not args.no_solve and world == 1:
+        solve = {}
+        del x, y
+        torch.cuda.empty_cache()
+        for name, prec, eps in (("fp64", sbd_tpb.FP64, 1e-6), ("mixed", sbd_tpb.MIXED, 1e-4)):
+            p = sbd_tpb.default_params(max_it=30, max_nb=8, eps=eps, precision=prec)
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            r = h.davidson(p, want_vector=False)
+            solve[name] = {"seconds": time.perf_counter() - ts, "sigma_steps": r["iterations"],
+                           "energy": r["energy"], "residual": r["residual"],
+                           "converged": r["converged"], "eps": eps}
+        solve["mixed"]["abs_energy_error_vs_fp64"] = abs(solve["mixed"]["energy"] - solve["fp64"]["energy"])
+        solve["speedup_mixed_vs_fp64"] = solve["fp64"]["seconds"] / solve["mixed"]["seconds"]
+        solve["note"] = "learned preconditioner not yet in this measurement (mixed + diagonal)"
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_reference_sigma(args.workload, args.cpu_sample_seconds)
+        if r is not None:
+            t = sum(r["sigma_s"]) / len(r["sigma_s"])
+            cpu = {"value": r["ndet"] / t / 1e9, "unit": "GDets/s", "cores": r["threads"],
+                   "kind": "reference",
+                   "sample": f"first {r['amax']} of {r['nstrings']} alpha x all beta strings "
+                             f"({r['ndet']} dets), one reference sbd::mult (tpb/mult.h:625-881)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GDets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 vectors, f64 accumulate" if dt == torch.float32 else "f64",
+            "data": "synthetic (seeded integrals 1729, strings 137)",
+            "config": {"workload": f"{args.workload}: norb={L}, {n}+{n} electrons, {cnt} x {cnt} strings",
+                       "determinants": N, "precision": args.precision,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (vector of %.2f GB)" % (N * esz / 1e9),
+                       "tables_s": t_tables, "setup_s": t1 - t0},
+            "gpu_launches": launches, "clocks": clocks.summary(), "roofline": roofline, "e2e": e2e,
+            "cpu_baseline": cpu, "time_to_solution": solve,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

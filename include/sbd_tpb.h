@@ -142,6 +142,14 @@ SBD_TPB_API int sbd_tpb_sigma(sbd_tpb_handle *h, const double *C, double *sigma,
 /* FP32 vectors (mixed-precision path), same semantics. */
 SBD_TPB_API int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigma, int accumulate, int mem);
 
+/* Device-vector sigma with an explicit sign convention, for callers that keep their vectors in
+ * HBM (their own eigensolver, benchmarks).  dtype 0 = double, 1 = float; convention 0 = the
+ * reference's (interleaved determinant, as sbd_tpb_sigma), 1 = the library's internal separated
+ * convention (alpha creators before beta creators: x_sep = D x_ref with
+ * D = (-1)^#{(p in Ia, q in Ib) : q < p}), which skips the two sign passes.  Same accumulate rule. */
+SBD_TPB_API int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
+                                     int accumulate, int convention);
+
 /* Davidson (tpb/davidson.h:667-930; basic/davidson_thrust.h:85-373) on the handle's problem,
  * from W (host, [na*nb], reference convention; NULL = HF start).  Writes the energy etc. into
  * result (ci_vector/density/RDM fields as in sbd_tpb_diag). */
@@ -158,6 +166,11 @@ SBD_TPB_API void *sbd_tpb_stream(sbd_tpb_handle *h);
 
 /* Timing of the last sigma call on the handle's stream (CUDA events), milliseconds. */
 SBD_TPB_API double sbd_tpb_last_sigma_ms(sbd_tpb_handle *h);
+
+/* Per-kernel device times (ms) of the last sigma call, in launch order: [0] row kernel
+ * (diagonal, beta part, alpha-beta part), [1] alpha column-slab kernel.  Returns how many were
+ * written (<= max_n) or a negative status. */
+SBD_TPB_API int sbd_tpb_last_sigma_kernels(sbd_tpb_handle *h, double *ms, int max_n);
 
 /* Number of kernel launches the library has issued on this handle (for accounting). */
 SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);

@@ -105,8 +105,9 @@ int sbd_tpb_create(int device, sbd_tpb_handle **out) {
   h->device = device;
   h->num_sms = prop.multiProcessorCount;
   h->smem_optin = prop.sharedMemPerBlockOptin;
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+  bool ev_ok = cudaEventCreate(&h->ev0) == cudaSuccess && cudaEventCreate(&h->ev1) == cudaSuccess;
+  for (cudaEvent_t &e : h->ev_k) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess || !ev_ok) {
     delete h;
     return fail(SBD_TPB_ERR_CUDA, "stream/event creation failed");
   }
@@ -121,6 +122,8 @@ int sbd_tpb_destroy(sbd_tpb_handle *h) {
   free_device_problem(h);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t e : h->ev_k)
+    if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return SBD_TPB_OK;
@@ -309,6 +312,24 @@ int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigma, int accum
   return SBD_TPB_OK;
 }
 
+int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtype, int accumulate,
+                         int convention) {
+  TPB_HANDLE(h);
+  if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
+  if (!C || !sigma) return fail(SBD_TPB_ERR_INVALID, "null vector");
+  if (dtype != 0 && dtype != 1) return fail(SBD_TPB_ERR_INVALID, "dtype must be 0 (double) or 1 (float)");
+  if (convention == 0) {
+    return dtype == 0 ? sbd_tpb_sigma(h, (const double *)C, (double *)sigma, accumulate, SBD_TPB_DEVICE)
+                      : sbd_tpb_sigma_f32(h, (const float *)C, (float *)sigma, accumulate, SBD_TPB_DEVICE);
+  }
+  if (convention != 1) return fail(SBD_TPB_ERR_INVALID, "convention must be 0 or 1");
+  if (dtype == 0) TPB_CHECK(sigma_sep<double>(h, (const double *)C, (double *)sigma, accumulate));
+  else TPB_CHECK(sigma_sep<float>(h, (const float *)C, (float *)sigma, accumulate));
+  TPB_CUDA(cudaEventSynchronize(h->ev1));
+  TPB_CUDA(cudaEventElapsedTime(&h->last_sigma_ms, h->ev0, h->ev1));
+  return SBD_TPB_OK;
+}
+
 int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params, const double *W0,
                      sbd_tpb_result *result) {
   TPB_HANDLE(h);
@@ -367,6 +388,21 @@ int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
 void *sbd_tpb_stream(sbd_tpb_handle *h) { return h ? (void *)h->stream : nullptr; }
 
 double sbd_tpb_last_sigma_ms(sbd_tpb_handle *h) { return h ? (double)h->last_sigma_ms : 0.0; }
+
+int sbd_tpb_last_sigma_kernels(sbd_tpb_handle *h, double *ms, int max_n) {
+  if (!h || !ms) return fail(SBD_TPB_ERR_INVALID, "null handle/output");
+  TPB_CHECK(use_device(h));
+  const int n = std::min(h->sigma_kernels, max_n);
+  cudaEvent_t prev = h->ev0;
+  for (int k = 0; k < n; k++) {
+    float t = 0.f;
+    TPB_CUDA(cudaEventSynchronize(h->ev_k[k]));
+    TPB_CUDA(cudaEventElapsedTime(&t, prev, h->ev_k[k]));
+    ms[k] = t;
+    prev = h->ev_k[k];
+  }
+  return n;
+}
 
 uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h) { return h ? h->launches : 0; }
 

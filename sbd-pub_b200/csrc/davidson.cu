@@ -11,8 +11,9 @@
 // Vectors live in HBM in the separated sign convention.  The FP64 path keeps everything in
 // double.  The mixed path stores C/HC/W/t in FP32, computes sigma of (H - s) with s = H_00 so the
 // FP32 entries carry residual-sized values, keeps all dot products and the Rayleigh-Ritz in FP64,
-// orthogonalises twice (classical Gram-Schmidt, two rounds), and finishes with one FP64 sigma on
-// the converged vector for the reported energy and residual.
+// and finishes with one FP64 sigma on the converged vector for the reported energy and residual.
+// Both orthogonalise with two rounds of classical Gram-Schmidt (as stable as the reference's
+// modified Gram-Schmidt, tpb/davidson.h:871-879, with two fused passes instead of k+1).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -258,7 +259,7 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
     TPB_CUDA(cudaMemcpy(&h00, h->d_hii, sizeof(double), cudaMemcpyDeviceToHost));
     TPB_CHECK(run_typed<float>(h, p, W0, h00, 2, res, Wsep, &resid, &nsig, &conv));
   } else {
-    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, 1, res, Wsep, &resid, &nsig, &conv));
+    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, 2, res, Wsep, &resid, &nsig, &conv));
   }
   // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
   double *dW = nullptr, *dHW = nullptr;

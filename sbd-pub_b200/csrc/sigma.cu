@@ -275,6 +275,8 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
     sigma_row_kernel<T, false><<<na, kRowThreads, smem, h->stream>>>(ra, C, sigma);
   }
   TPB_LAUNCHED(h);
+  TPB_CUDA(cudaEventRecord(h->ev_k[0], h->stream));
+  h->sigma_kernels = 1;
   if (h->pa.nnz > 0) {
     SlabArgs sa;
     sa.bstr = h->d_bstr;
@@ -292,6 +294,8 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
     if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
     sigma_alpha_slab_kernel<T><<<(unsigned)blocks, kSlabThreads, 0, h->stream>>>(sa, C, sigma);
     TPB_LAUNCHED(h);
+    TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
+    h->sigma_kernels = 2;
   }
   TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
   return SBD_TPB_OK;

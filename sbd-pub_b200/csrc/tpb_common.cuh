@@ -115,8 +115,10 @@ struct sbd_tpb_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_k[4] = {nullptr, nullptr, nullptr, nullptr};  // between sigma kernels
   uint64_t launches = 0;
   float last_sigma_ms = 0.f;
+  int sigma_kernels = 0;  // kernels timed in the last sigma (ev0, ev_k[0..], ev1)
   int num_sms = 148;
   size_t smem_optin = 0;
 

@@ -37,8 +37,8 @@ EXPORTED = [
     "sbd_tpb_default_params", "sbd_tpb_diag", "sbd_tpb_last_error", "sbd_tpb_create",
     "sbd_tpb_destroy", "sbd_tpb_set_hamiltonian", "sbd_tpb_set_strings", "sbd_tpb_build_tables",
     "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
-    "sbd_tpb_sigma_f32", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
-    "sbd_tpb_last_sigma_ms", "sbd_tpb_kernel_launches",
+    "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
+    "sbd_tpb_last_sigma_ms", "sbd_tpb_last_sigma_kernels", "sbd_tpb_kernel_launches",
 ]
 
 
@@ -101,12 +101,14 @@ def lib():
     L.sbd_tpb_diagonal.argtypes = [vp, vp, C.c_int]
     L.sbd_tpb_sigma.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.sbd_tpb_sigma_f32.argtypes = [vp, vp, vp, C.c_int, C.c_int]
+    L.sbd_tpb_sigma_device.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int]
     L.sbd_tpb_davidson.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
     L.sbd_tpb_rdm.argtypes = [vp, vp, vp, vp, C.c_int]
     L.sbd_tpb_stream.restype = vp
     L.sbd_tpb_stream.argtypes = [vp]
     L.sbd_tpb_last_sigma_ms.restype = C.c_double
     L.sbd_tpb_last_sigma_ms.argtypes = [vp]
+    L.sbd_tpb_last_sigma_kernels.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
     L.sbd_tpb_kernel_launches.restype = C.c_uint64
     L.sbd_tpb_kernel_launches.argtypes = [vp]
     _lib = L
@@ -220,8 +222,22 @@ class Handle:
         _check(fn(self.h, _ptr(C_), _ptr(out), int(accumulate), DEVICE if dev else HOST))
         return out
 
+    def sigma_device(self, x, y, accumulate=False, separated=True):
+        """sigma on torch CUDA tensors; separated=True keeps the library's internal convention."""
+        dt = 1 if str(x.dtype) == "torch.float32" else 0
+        _check(lib().sbd_tpb_sigma_device(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate),
+                                          1 if separated else 0))
+        return y
+
     def last_sigma_ms(self) -> float:
         return lib().sbd_tpb_last_sigma_ms(self.h)
+
+    def last_sigma_kernels(self):
+        """Device ms of each kernel of the last sigma: [row kernel, alpha slab kernel]."""
+        buf = (C.c_double * 8)()
+        n = lib().sbd_tpb_last_sigma_kernels(self.h, buf, 8)
+        _check(n if n < 0 else OK)
+        return [buf[i] for i in range(n)]
 
     def kernel_launches(self) -> int:
         return int(lib().sbd_tpb_kernel_launches(self.h))
