@@ -14,7 +14,10 @@
 //   beta pairs    the same on the transposed vector
 //   alpha x beta  X(e, rs) = sum_{beta singles with label rs} s_b W[Ia,Ib] W[Ja,Jb]
 // Signs are those of the separated convention, in which the vector W also lives, so the RDMs
-// equal the reference's.
+// equal the reference's.  Same-spin blocks are the physical <c+ c+ c c> above; the opposite-spin
+// blocks of alpha-single x beta-single pairs follow the reference's placement rule, which puts
+// a pair's value in the [s+2t] block chosen by the spin-orbital ordering of its four indices
+// (basic/correlation.h:191-231), so the spin-resolved arrays match it entry by entry.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -380,9 +383,20 @@ int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double
             if (xr[rs] == 0.0) continue;
             const int crb = rs / L, anb = rs % L;
             const double x = sa * xr[rs];
-            // <c+_{cra a} c+_{crb b} c_{anb b} c_{ana a}> = sa * sb
-            R.G(0, 1, cra, crb, ana, anb) += x;
-            R.G(1, 0, crb, cra, anb, ana) += x;
+            // placement of TwoDiffCorrelation for an alpha-single x beta-single pair
+            // (basic/correlation.h:191-231): spin-orbitals ordered I<J (bra), A<B (ket); the
+            // value is the separated-convention sign sa*sb times W_bra W_ket in either branch
+            const int i = 2 * cra, j = 2 * crb + 1, a = 2 * ana, b = 2 * anb + 1;
+            const int I = std::min(i, j), J = std::max(i, j), A = std::min(a, b), B = std::max(a, b);
+            const int oi = I / 2, si = I % 2, oj = J / 2, sj = J % 2, oa = A / 2, sa_ = A % 2,
+                      ob = B / 2;
+            if (si == sa_) {
+              R.G(si, sj, oa, ob, oi, oj) += x;
+              R.G(sj, si, ob, oa, oj, oi) += x;
+            } else {
+              R.G(si, sj, oa, ob, oj, oi) += x;
+              R.G(sj, si, ob, oa, oi, oj) += x;
+            }
           }
         }
     }

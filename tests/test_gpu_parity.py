@@ -157,7 +157,7 @@ def test_invalid_inputs_return_status(tpb):
     with pytest.raises(tpb.TpbError) as e:
         h.set_problem(wide)
     assert e.value.code == tpb.ERR_INVALID
-    mixed = type(prob)(**{**prob.__dict__, "astr": np.array([0b111, 0b1011], np.uint64)})
+    mixed = type(prob)(**{**prob.__dict__, "astr": np.array([0b111, 0b1111], np.uint64)})
     with pytest.raises(tpb.TpbError) as e:
         h.set_problem(mixed)
     assert "electron count" in str(e.value)
