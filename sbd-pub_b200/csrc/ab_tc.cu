@@ -1,0 +1,326 @@
+// Split-BF16 tcgen05 contraction for the dense alpha-beta path of the FP32 (mixed) sigma.
+//
+//   E[n][j] = sum_k V[n][k] D[j][k],  D ~ Dhi + Dlo,  V ~ Vhi + Vlo  (BF16 parts)
+//   E ~ Dhi.Vhi + Dhi.Vlo + Dlo.Vhi   with FP32 accumulation in tensor memory.
+//
+// One persistent CTA per SM (128 threads).  The V operand (alpha labels x beta labels) stays in
+// shared memory for the whole kernel; for each 128-row tile of D one thread issues a 1-D bulk
+// copy (cp.async.bulk, completion on an mbarrier) of the hi and lo parts -- the gather kernel
+// already wrote each tile in the canonical K-major, no-swizzle layout tcgen05.mma reads (8x8
+// core matrices of 128 B; k-groups 2 KB apart) -- then issues 3 x Kp/16 tcgen05.mma
+// (cta_group::1, kind::f16, M=128, N<=256 per instruction) into an FP32 accumulator in TMEM and
+// commits to a second mbarrier; the four warps read their 32 accumulator lanes back with
+// tcgen05.ld and store E label-major (coalesced along the determinant index).  Every mbarrier
+// wait is bounded; on timeout the kernel records an error code, waits (bounded) for copies in
+// flight, releases its TMEM and returns, and the host reports the failure.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "ab_tc.cuh"
+
+namespace sbdtpb {
+namespace {
+
+constexpr long long kWaitLimit = 1ll << 24;
+
+__host__ __device__ __forceinline__ size_t tiled_off(size_t j, int k, int Kp) {
+  const size_t t = j >> 7;
+  const int r = (int)(j & 127);
+  return t * (size_t)128 * Kp + ((size_t)((k >> 3) * 16 + (r >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+
+__host__ __device__ __forceinline__ size_t tiled_off_b(int n, int k, int Np) {
+  const int NG = Np >> 3;
+  return ((size_t)((k >> 3) * NG + (n >> 3)) << 6) + ((n & 7) << 3) + (k & 7);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100; no swizzle, base offset 0
+  return d;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(addr), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+  for (long long i = 0; i < kWaitLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared memory: [Bhi Np*Kp][Blo Np*Kp][Ahi 128*Kp][Alo 128*Kp] (bf16) | mbar_load | mbar_mma |
+// tmem base | status
+__global__ void __launch_bounds__(128, 1)
+    ab_tc_kernel(const __nv_bfloat16 *__restrict__ Ahi, const __nv_bfloat16 *__restrict__ Alo,
+                 const __nv_bfloat16 *__restrict__ Bhi, const __nv_bfloat16 *__restrict__ Blo,
+                 float *__restrict__ E, int Kp, int Np, int npq, size_t M, size_t ntiles,
+                 int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const uint32_t b_bytes = (uint32_t)Np * Kp * 2, a_bytes = 128u * Kp * 2;
+  unsigned char *sBhi = smem, *sBlo = smem + b_bytes, *sAhi = smem + 2 * b_bytes,
+                *sAlo = smem + 2 * b_bytes + a_bytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * b_bytes + 2 * a_bytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
+  volatile int *status = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  const uint32_t bar_load = smem_addr(&bars[0]), bar_mma = smem_addr(&bars[1]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t ncols = 32;
+  while ((int)ncols < Np) ncols <<= 1;
+
+  if (threadIdx.x == 0) {
+    mbar_init(bar_load, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    *status = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  // idesc: D F32 (bits 4-5 = 1), A/B BF16 (bits 7-9, 10-12 = 1), K-major A/B, M = 128 (bits 24-28)
+  uint32_t load_phase = 0, mma_phase = 0;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar_load, 2 * b_bytes);
+    bulk_g2s(smem_addr(sBhi), Bhi, b_bytes, bar_load);
+    bulk_g2s(smem_addr(sBlo), Blo, b_bytes, bar_load);
+    if (!mbar_wait(bar_load, load_phase)) {
+      atomicExch(err, 1);
+      *status = 1;
+      mbar_wait(bar_load, load_phase);  // bounded second wait for the copies in flight
+    }
+    load_phase ^= 1;
+  }
+  __syncthreads();
+
+  const int NG = Np >> 3;
+  for (size_t tile = blockIdx.x; tile < ntiles && *status == 0; tile += gridDim.x) {
+    if (threadIdx.x == 0) {
+      const size_t off = tile * (size_t)128 * Kp;
+      mbar_expect_tx(bar_load, 2 * a_bytes);
+      bulk_g2s(smem_addr(sAhi), Ahi + off, a_bytes, bar_load);
+      bulk_g2s(smem_addr(sAlo), Alo + off, a_bytes, bar_load);
+      bool ok = mbar_wait(bar_load, load_phase);
+      load_phase ^= 1;
+      if (!ok) {
+        atomicExch(err, 2);
+        *status = 1;
+        mbar_wait(bar_load, load_phase ^ 1);
+      } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_addr(sAhi), a1 = smem_addr(sAlo);
+        const uint32_t b0 = smem_addr(sBhi), b1 = smem_addr(sBlo);
+        for (int c = 0; c * 256 < Np; c++) {
+          const int nc = min(256, Np - c * 256);
+          const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nc >> 3) << 17) |
+                                 ((uint32_t)(128 >> 4) << 24);
+          const uint32_t td = tmem + (uint32_t)(c * 256);
+          for (int s = 0; s < Kp / 16; s++) {
+            const uint32_t aoff = (uint32_t)(2 * s) * 2048u;
+            const uint32_t boff = (uint32_t)((2 * s) * NG + 32 * c) * 128u;
+            const uint64_t dah = make_desc(a0 + aoff, 2048u, 128u);
+            const uint64_t dal = make_desc(a1 + aoff, 2048u, 128u);
+            const uint64_t dbh = make_desc(b0 + boff, (uint32_t)NG * 128u, 128u);
+            const uint64_t dbl = make_desc(b1 + boff, (uint32_t)NG * 128u, 128u);
+            mma_bf16(td, dah, dbh, idesc, s > 0 ? 1u : 0u);
+            mma_bf16(td, dah, dbl, idesc, 1u);
+            mma_bf16(td, dal, dbh, idesc, 1u);
+          }
+        }
+        mma_commit(bar_mma);
+        ok = mbar_wait(bar_mma, mma_phase);
+        mma_phase ^= 1;
+        if (!ok) {
+          atomicExch(err, 3);
+          *status = 1;
+        }
+      }
+    }
+    __syncthreads();
+    if (*status != 0) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const size_t j = tile * 128 + (size_t)warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int col = 0; col < Np; col += 16) {
+      float v[16];
+      tmem_ld16(trow + (uint32_t)col, v);
+      if (j < M) {
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+          if (col + i < npq) E[(size_t)(col + i) * M + j] = v[i];
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
+__global__ void ab_tc_gather_kernel(const float *__restrict__ C, uint32_t na, uint32_t nb,
+                                    const uint32_t *__restrict__ b_off, const uint32_t *__restrict__ b_ket,
+                                    const int32_t *__restrict__ b_label, int Kp,
+                                    __nv_bfloat16 *__restrict__ Dhi, __nv_bfloat16 *__restrict__ Dlo) {
+  const size_t total = (size_t)na * nb;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < total;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t ja = (uint32_t)(j / nb), ib = (uint32_t)(j - (size_t)ja * nb);
+    const float *crow = C + (size_t)ja * nb;
+    for (uint32_t e = b_off[ib]; e < b_off[ib + 1]; e++) {
+      const int32_t lab = b_label[e];
+      float x = crow[b_ket[e]];
+      if (lab < 0) x = -x;
+      const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+      const size_t o = tiled_off(j, (lab > 0 ? lab : -lab) - 1, Kp);
+      Dhi[o] = hi;
+      Dlo[o] = lo;
+    }
+  }
+}
+
+}  // namespace
+
+int ab_tc_setup(sbd_tpb_handle *h) {
+  ABDense &ab = h->ab;
+  ab.tc_ready = false;
+  const int Kp = (ab.nrs + 15) / 16 * 16, Np = (ab.npq + 15) / 16 * 16;
+  const size_t smem = (size_t)2 * Np * Kp * 2 + (size_t)2 * 128 * Kp * 2 + 64;
+  if (Np > 512 || smem > h->smem_optin) return SBD_TPB_OK;  // CUDA-core contraction instead
+  ab.Kp = Kp;
+  ab.Np = Np;
+  std::vector<double> V((size_t)ab.npq * ab.nrs);
+  TPB_CUDA(cudaMemcpy(V.data(), ab.V, sizeof(double) * V.size(), cudaMemcpyDeviceToHost));
+  std::vector<__nv_bfloat16> hi((size_t)Np * Kp, __float2bfloat16(0.f)), lo = hi;
+  for (int n = 0; n < ab.npq; n++)
+    for (int k = 0; k < ab.nrs; k++) {
+      const float x = (float)V[(size_t)n * ab.nrs + k];
+      const __nv_bfloat16 xh = __float2bfloat16_rn(x);
+      hi[tiled_off_b(n, k, Np)] = xh;
+      lo[tiled_off_b(n, k, Np)] = __float2bfloat16_rn(x - __bfloat162float(xh));
+    }
+  TPB_CUDA(cudaMalloc(&ab.Vhi, sizeof(uint16_t) * hi.size()));
+  TPB_CUDA(cudaMalloc(&ab.Vlo, sizeof(uint16_t) * lo.size()));
+  TPB_CUDA(cudaMemcpy(ab.Vhi, hi.data(), sizeof(uint16_t) * hi.size(), cudaMemcpyHostToDevice));
+  TPB_CUDA(cudaMemcpy(ab.Vlo, lo.data(), sizeof(uint16_t) * lo.size(), cudaMemcpyHostToDevice));
+  if (!ab.err) TPB_CUDA(cudaMalloc(&ab.err, sizeof(int)));
+  TPB_CUDA(cudaMemset(ab.err, 0, sizeof(int)));
+  TPB_CUDA(cudaFuncSetAttribute(ab_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ab.tc_ready = true;
+  return SBD_TPB_OK;
+}
+
+size_t ab_tc_work_bytes(sbd_tpb_handle *h) {
+  const ABDense &ab = h->ab;
+  const size_t M = h->ndet(), Mp = (M + 127) / 128 * 128;
+  return Mp * ab.Kp * 2 * sizeof(uint16_t) + M * (size_t)ab.npq * sizeof(float);
+}
+
+int ab_tc_gather(sbd_tpb_handle *h, const float *C, size_t M) {
+  ABDense &ab = h->ab;
+  const size_t Mp = (M + 127) / 128 * 128;
+  __nv_bfloat16 *Dhi = reinterpret_cast<__nv_bfloat16 *>(h->d_ab_work);
+  __nv_bfloat16 *Dlo = Dhi + Mp * ab.Kp;
+  TPB_CUDA(cudaMemsetAsync(Dhi, 0, sizeof(uint16_t) * Mp * ab.Kp * 2, h->stream));
+  ab_tc_gather_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(
+      C, (uint32_t)h->astr.size(), (uint32_t)h->bstr.size(), h->tb_s.off, h->tb_s.ket, ab.b_label,
+      ab.Kp, Dhi, Dlo);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+int ab_tc_gemm(sbd_tpb_handle *h, const float *, float *E, size_t M) {
+  ABDense &ab = h->ab;
+  const size_t Mp = (M + 127) / 128 * 128, ntiles = Mp / 128;
+  const __nv_bfloat16 *Dhi = reinterpret_cast<const __nv_bfloat16 *>(h->d_ab_work);
+  const __nv_bfloat16 *Dlo = Dhi + Mp * ab.Kp;
+  const size_t smem = (size_t)2 * ab.Np * ab.Kp * 2 + (size_t)2 * 128 * ab.Kp * 2 + 64;
+  const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)h->num_sms);
+  ab_tc_kernel<<<grid, 128, smem, h->stream>>>(Dhi, Dlo, reinterpret_cast<const __nv_bfloat16 *>(ab.Vhi),
+                                               reinterpret_cast<const __nv_bfloat16 *>(ab.Vlo), E,
+                                               ab.Kp, ab.Np, ab.npq, M, ntiles, ab.err);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+int ab_tc_check(sbd_tpb_handle *h) {
+  if (!h->ab.err) return SBD_TPB_OK;
+  int e = 0;
+  TPB_CUDA(cudaMemcpy(&e, h->ab.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(h->ab.err, 0, sizeof(int));
+    return fail(SBD_TPB_ERR_CUDA, "alpha-beta tensor-core kernel: bounded wait expired (code " +
+                                      std::to_string(e) + ")");
+  }
+  return SBD_TPB_OK;
+}
+
+}  // namespace sbdtpb

@@ -208,6 +208,7 @@ int sbd_tpb_build_tables(sbd_tpb_handle *h) {
   TPB_CHECK(build_excitation_tables(h));
   TPB_CHECK(build_sigma_programs(h));
   TPB_CHECK(compute_diagonal(h));
+  TPB_CHECK(ab_dense_setup(h, ab_dense_worthwhile(h) ? 1 : 0));
   TPB_CUDA(cudaStreamSynchronize(h->stream));
   h->have_tables = true;
   return SBD_TPB_OK;

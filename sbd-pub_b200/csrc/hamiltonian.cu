@@ -55,28 +55,21 @@ __global__ void diag_kernel(const uint64_t *__restrict__ astr, const uint64_t *_
   }
 }
 
-// One warp per bra row: write singles then doubles of the row into the program, with values.
-__global__ void program_kernel(const uint64_t *__restrict__ str, uint32_t n, int L,
-                               const uint32_t *__restrict__ s_off,
-                               const uint32_t *__restrict__ s_ket,
-                               const uint32_t *__restrict__ s_lab,
-                               const uint32_t *__restrict__ d_off,
-                               const uint32_t *__restrict__ d_ket,
-                               const uint32_t *__restrict__ d_lab, const double *__restrict__ eri,
-                               const double *__restrict__ h1, const uint32_t *__restrict__ p_off,
-                               uint32_t *__restrict__ p_ket, double *__restrict__ p_val,
-                               float *__restrict__ p_valf, int32_t *__restrict__ p_pair) {
+// Values of the sigma program, aligned entry by entry with the excitation tables.
+__global__ void single_values_kernel(const uint64_t *__restrict__ str, uint32_t n, int L,
+                                     const uint32_t *__restrict__ off,
+                                     const uint32_t *__restrict__ lab,
+                                     const double *__restrict__ eri, const double *__restrict__ h1,
+                                     double *__restrict__ val, float *__restrict__ valf,
+                                     int32_t *__restrict__ pairsgn) {
   const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
   const uint64_t I = str[row];
   const size_t L2 = (size_t)L * L;
-  const uint32_t s0 = s_off[row], s1 = s_off[row + 1];
-  const uint32_t d0 = d_off[row], d1 = d_off[row + 1];
-  const uint32_t out0 = p_off[row];
-  for (uint32_t e = s0 + lane; e < s1; e += 32) {
-    const uint32_t lab = s_lab[e];
-    const int cr = lab & 0xff, an = (lab >> 8) & 0xff;
+  for (uint32_t e = off[row] + lane; e < off[row + 1]; e += 32) {
+    const uint32_t lb = lab[e];
+    const int cr = lb & 0xff, an = (lb >> 8) & 0xff;
     const int lo = min(cr, an), hi = max(cr, an);
     const double sgn = (__popcll(I & open_mask(lo, hi)) & 1) ? -1.0 : 1.0;
     double v = h1[(size_t)an * L + cr];
@@ -87,71 +80,63 @@ __global__ void program_kernel(const uint64_t *__restrict__ str, uint32_t n, int
            eri[((size_t)an * L + j) * L2 + (size_t)j * L + cr];
       occ &= occ - 1;
     }
-    const uint32_t o = out0 + (e - s0);
-    p_ket[o] = s_ket[e];
-    p_val[o] = sgn * v;
-    p_valf[o] = (float)(sgn * v);
-    p_pair[o] = (sgn < 0 ? -1 : 1) * (an * L + cr + 1);
+    val[e] = sgn * v;
+    valf[e] = (float)(sgn * v);
+    pairsgn[e] = (sgn < 0 ? -1 : 1) * (an * L + cr + 1);
   }
-  for (uint32_t e = d0 + lane; e < d1; e += 32) {
-    const uint32_t lab = d_lab[e];
-    const int I0 = lab & 0xff, J0 = (lab >> 8) & 0xff, A0 = (lab >> 16) & 0xff,
-              B0 = (lab >> 24) & 0xff;
+}
+
+__global__ void double_values_kernel(const uint64_t *__restrict__ str, uint32_t n, int L,
+                                     const uint32_t *__restrict__ off,
+                                     const uint32_t *__restrict__ lab,
+                                     const double *__restrict__ eri, double *__restrict__ val,
+                                     float *__restrict__ valf) {
+  const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const uint64_t I = str[row];
+  const size_t L2 = (size_t)L * L;
+  for (uint32_t e = off[row] + lane; e < off[row + 1]; e += 32) {
+    const uint32_t lb = lab[e];
+    const int I0 = lb & 0xff, J0 = (lb >> 8) & 0xff, A0 = (lb >> 16) & 0xff, B0 = (lb >> 24) & 0xff;
     int par = __popcll(I & open_mask(min(I0, A0), max(I0, A0))) +
               __popcll(I & open_mask(min(J0, B0), max(J0, B0)));
     if (A0 > J0 || B0 < I0) par += 1;
     const double sgn = (par & 1) ? -1.0 : 1.0;
     const double v = eri[((size_t)A0 * L + I0) * L2 + (size_t)B0 * L + J0] -
                      eri[((size_t)A0 * L + J0) * L2 + (size_t)B0 * L + I0];
-    const uint32_t o = out0 + (s1 - s0) + (e - d0);
-    p_ket[o] = d_ket[e];
-    p_val[o] = sgn * v;
-    p_valf[o] = (float)(sgn * v);
-    p_pair[o] = 0;
+    val[e] = sgn * v;
+    valf[e] = (float)(sgn * v);
   }
 }
 
-__global__ void add_offsets_kernel(const uint32_t *__restrict__ a, const uint32_t *__restrict__ b,
-                                   uint32_t n, uint32_t *__restrict__ out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
-    out[i] = a[i] + b[i];
-}
-
 void free_prog(SigmaProg &p) {
-  free_dev(p.off);
-  free_dev(p.ket);
-  free_dev(p.val);
-  free_dev(p.valf);
-  free_dev(p.pairsgn);
+  free_dev(p.s_val);
+  free_dev(p.s_valf);
+  free_dev(p.s_pair);
+  free_dev(p.d_val);
+  free_dev(p.d_valf);
   p = SigmaProg();
 }
 
 int build_prog(sbd_tpb_handle *h, const uint64_t *d_str, uint32_t n, const ExTable &ts,
                const ExTable &td, const double *h1dev, SigmaProg &p) {
   free_prog(p);
-  p.nnz = ts.nnz + td.nnz;
-  if (p.nnz >= 0xffffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma program exceeds 2^32 entries");
-  const size_t m = p.nnz ? p.nnz : 1;
-  TPB_CUDA(cudaMalloc(&p.off, sizeof(uint32_t) * (n + 1)));
-  TPB_CUDA(cudaMalloc(&p.ket, sizeof(uint32_t) * m));
-  TPB_CUDA(cudaMalloc(&p.val, sizeof(double) * m));
-  TPB_CUDA(cudaMalloc(&p.valf, sizeof(float) * m));
-  TPB_CUDA(cudaMalloc(&p.pairsgn, sizeof(int32_t) * m));
-  add_offsets_kernel<<<std::max(1u, std::min(1024u, (n + 256) / 256)), 256, 0, h->stream>>>(
-      ts.off, td.off, n, p.off);
+  const size_t ms = ts.nnz ? ts.nnz : 1, md = td.nnz ? td.nnz : 1;
+  TPB_CUDA(cudaMalloc(&p.s_val, sizeof(double) * ms));
+  TPB_CUDA(cudaMalloc(&p.s_valf, sizeof(float) * ms));
+  TPB_CUDA(cudaMalloc(&p.s_pair, sizeof(int32_t) * ms));
+  TPB_CUDA(cudaMalloc(&p.d_val, sizeof(double) * md));
+  TPB_CUDA(cudaMalloc(&p.d_valf, sizeof(float) * md));
+  const unsigned grid = (n + 7) / 8;
+  single_values_kernel<<<grid, 256, 0, h->stream>>>(d_str, n, h->L, ts.off, ts.lab, h->d_eri, h1dev,
+                                                   p.s_val, p.s_valf, p.s_pair);
   TPB_LAUNCHED(h);
-  program_kernel<<<(n + 7) / 8, 256, 0, h->stream>>>(d_str, n, h->L, ts.off, ts.ket, ts.lab,
-                                                     td.off, td.ket, td.lab, h->d_eri, h1dev,
-                                                     p.off, p.ket, p.val, p.valf, p.pairsgn);
+  double_values_kernel<<<grid, 256, 0, h->stream>>>(d_str, n, h->L, td.off, td.lab, h->d_eri,
+                                                   p.d_val, p.d_valf);
   TPB_LAUNCHED(h);
-  // longest row, for the kernels' shared-memory staging
-  std::vector<uint32_t> off(n + 1);
-  TPB_CUDA(cudaMemcpyAsync(off.data(), p.off, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost,
-                           h->stream));
-  TPB_CUDA(cudaStreamSynchronize(h->stream));
-  uint32_t mx = 0;
-  for (uint32_t i = 0; i < n; i++) mx = std::max(mx, off[i + 1] - off[i]);
-  p.max_row = mx;
+  p.s = &ts;
+  p.d = &td;
   return SBD_TPB_OK;
 }
 
@@ -181,8 +166,10 @@ void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->ab.a_label);
   free_dev(h->ab.b_label);
   free_dev(h->ab.V);
+  free_dev(h->ab.Vf);
   free_dev(h->ab.Vhi);
   free_dev(h->ab.Vlo);
+  free_dev(h->ab.err);
   h->ab = ABDense();
   free_dev(h->d_partials);
   h->partials_cap = 0;

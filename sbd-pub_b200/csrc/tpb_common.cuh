@@ -82,31 +82,34 @@ struct ExTable {
   uint32_t max_row = 0;     // longest bra row
 };
 
-// One spin's sigma program: per bra string, singles then doubles, with the separated-convention
-// element.  For singles, pairsgn = +-(an*L + cr + 1) marks the other-spin Coulomb term
-// sgn * sum_{k in other string} (an cr|kk); 0 for doubles.
+// One spin's sigma program: the separated-convention matrix element of every excitation-table
+// entry, aligned with the table (same offsets and ket indices).  Singles carry, in s_pair,
+// +-(an*L + cr + 1): the sign of the element and the orbital pair of the other-spin Coulomb term
+// sgn * sum_{k in other string} (an cr|kk) that the sigma kernels add.
 struct SigmaProg {
-  uint32_t *off = nullptr;
-  uint32_t *ket = nullptr;
-  double *val = nullptr;
-  float *valf = nullptr;
-  int32_t *pairsgn = nullptr;
-  size_t nnz = 0;
-  uint32_t max_row = 0;  // longest row
+  const ExTable *s = nullptr, *d = nullptr;  // singles / doubles tables (offsets, kets)
+  double *s_val = nullptr;
+  float *s_valf = nullptr;
+  int32_t *s_pair = nullptr;
+  double *d_val = nullptr;
+  float *d_valf = nullptr;
 };
 
 // Dense-path data for the alpha-beta term as gather -> (pq|rs) contraction -> scatter.
 struct ABDense {
   bool enabled = false;
   int npq = 0, nrs = 0;           // distinct alpha / beta single labels
-  int *pq_of_label = nullptr;     // [npq] pair index p*L+q per label (device)
-  int *rs_of_label = nullptr;     // [nrs]
-  int32_t *a_label = nullptr;     // [nnz alpha singles] label id per entry (sign in bit 31)
-  int32_t *b_label = nullptr;     // [nnz beta singles]
-  uint32_t *a_off = nullptr, *a_ket = nullptr;  // alpha singles CSR (bra -> ket)
-  uint32_t *b_off = nullptr, *b_ket = nullptr;  // beta singles CSR
-  double *V = nullptr;            // [nrs][npq] (pq|rs), FP64
-  uint16_t *Vhi = nullptr, *Vlo = nullptr;  // split BF16 of V, K-major for the tensor-core path
+  int *pq_of_label = nullptr;     // unused placeholders kept for layout stability
+  int *rs_of_label = nullptr;
+  int32_t *a_label = nullptr;     // [alpha singles] +-(label+1), sign = s_a
+  int32_t *b_label = nullptr;     // [beta singles]  +-(label+1), sign = s_b
+  double *V = nullptr;            // [npq][nrs] (pq|rs), FP64
+  float *Vf = nullptr;            // same in FP32
+  // tensor-core path (FP32 sigma): V as BF16 hi/lo in the tcgen05 canonical layout
+  bool tc_ready = false;
+  int Kp = 0, Np = 0;
+  uint16_t *Vhi = nullptr, *Vlo = nullptr;
+  int *err = nullptr;             // bounded-wait status of the tensor-core kernel
 };
 
 }  // namespace sbdtpb
@@ -176,6 +179,7 @@ int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y);
 int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y);
 // ab_dense.cu: alpha-beta term as gather -> dense (pq|rs) contraction -> scatter
 int ab_dense_setup(sbd_tpb_handle *h, int enable);
+bool ab_dense_worthwhile(sbd_tpb_handle *h);
 template <typename T>
 int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma);
 // vecops.cu
