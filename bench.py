@@ -256,15 +256,15 @@ def run_ours(args, world, rank, local, pg):
         h.sigma_device(x, y)
         kern.append(h.last_sigma_kernels())
     kern = np.array(kern).mean(axis=0)
-    pa_nnz = sum(int(h.table(k)[1].size) for k in (0, 1))
-    pb_nnz = sum(int(h.table(k)[1].size) for k in (2, 3))
-    val_b = esz  # sigma element values are stored at the vector precision
-    tab_row = pb_nnz * (4 + val_b + 4) + 4 * (len(prob.bstr) + 1)
-    tab_slab = pa_nnz * (4 + val_b + 4) + 4 * (len(prob.astr) + 1)
-    bytes_row = N * esz + N * esz + N * 8 + tab_row       # read C, write sigma, read H_ii, tables
-    bytes_slab = N * esz + 2 * N * esz + tab_slab         # read C, sigma read-modify-write, tables
-    names = ["sigma_row_kernel", "sigma_alpha_slab_kernel"]
-    per = [bytes_row, bytes_slab]
+    # algorithmic bytes of each pass: 3 N s (alpha: read C, write sigma, write C^T; beta: read
+    # C^T, sigma read-modify-write) plus its sigma-program tables read once
+    def table_bytes(singles, doubles):
+        ns, nd = int(h.table(singles)[1].size), int(h.table(doubles)[1].size)
+        return ns * (4 + esz + 4) + nd * (4 + esz) + 8 * (len(prob.astr) + 1)
+    bytes_alpha = 3 * N * esz + table_bytes(0, 1)
+    bytes_beta = 3 * N * esz + table_bytes(2, 3)
+    names = ["sigma_block_kernel<alpha>", "sigma_block_kernel<beta>"]
+    per = [bytes_alpha, bytes_beta]
     dom = int(np.argmax(kern))
     pk = peaks()
     achieved = per[dom] / (kern[dom] * 1e-3) / 1e9

@@ -180,6 +180,9 @@ void free_device_problem(sbd_tpb_handle *h) {
   if (h->d_ab_work) cudaFree(h->d_ab_work);
   h->d_ab_work = nullptr;
   h->ab_work_bytes = 0;
+  if (h->d_ct) cudaFree(h->d_ct);
+  h->d_ct = nullptr;
+  h->ct_bytes = 0;
   h->have_tables = false;
 }
 

@@ -153,6 +153,8 @@ struct sbd_tpb_handle {
   double *d_tmp64 = nullptr;     // one N-vector FP64 (sign conversion staging)
   double *d_tmp64b = nullptr;
   float *d_tmp32 = nullptr, *d_tmp32b = nullptr;
+  void *d_ct = nullptr;          // C^T staging of the beta pass of sigma
+  size_t ct_bytes = 0;
   void *d_ab_work = nullptr;     // dense alpha-beta intermediates
   size_t ab_work_bytes = 0;
   size_t ndet() const { return astr.size() * bstr.size(); }
