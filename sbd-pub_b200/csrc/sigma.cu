@@ -22,7 +22,7 @@
 namespace sbdtpb {
 namespace {
 
-constexpr int kBlkRows = 32;     // bra rows per CTA
+constexpr int kBlkRows = 8;  // bra rows per CTA
 constexpr int kBlkThreads = 128;
 
 template <typename T>
@@ -35,6 +35,36 @@ template <>
 __device__ __forceinline__ float val_of<float>(const double *, const float *vf, uint32_t e) {
   return __ldg(&vf[e]);
 }
+
+// VW consecutive elements of type T: one 16-byte load when kVec, VW scalars otherwise.
+template <typename T, int VW, bool kVec>
+struct Vec;
+template <bool kVec>
+struct Vec<float, 4, kVec> {
+  float v[4];
+  __device__ __forceinline__ void load(const float *p) {
+    if (kVec) {
+      const float4 f = __ldg(reinterpret_cast<const float4 *>(p));
+      v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = __ldg(p + i);
+    }
+  }
+};
+template <bool kVec>
+struct Vec<double, 2, kVec> {
+  double v[2];
+  __device__ __forceinline__ void load(const double *p) {
+    if (kVec) {
+      const double2 f = __ldg(reinterpret_cast<const double2 *>(p));
+      v[0] = f.x, v[1] = f.y;
+    } else {
+      v[0] = __ldg(p);
+      v[1] = __ldg(p + 1);
+    }
+  }
+};
 
 struct BlockArgs {
   // sigma program of the bra spin (rows of X)
@@ -49,9 +79,10 @@ struct BlockArgs {
   const double *vd;         // (pq|kk) [L*L][L]
   int L;
   uint32_t nrows, ncols;    // X is nrows x ncols, row-major
-  // alpha pass only: on-the-fly diagonal, alpha-single x beta-single terms
-  double core_shift;        // I0 - shift
-  const double *Ea, *Eb, *uJ;
+  uint32_t max_d, max_s;    // most doubles / singles entries of any kBlkRows-row block
+  // alpha pass only: diagonal, alpha-single x beta-single terms
+  const double *hii;
+  double shift;
   int accumulate;
   int do_ab;
   const uint32_t *bs_off, *bs_ket;
@@ -59,75 +90,115 @@ struct BlockArgs {
   const double *eri;
 };
 
-// One kernel, two passes.  A CTA owns 32 consecutive bra strings (rows of X) and a slab of
-// kBlkThreads*CPT columns; blocks run slab-major so the CTAs in flight gather from one slab of X
-// that stays in L2.  For each of its rows a thread accumulates sum_ket H(row, ket) X[ket, col]
-// over its CPT columns.
-//   alpha pass (kAlpha): X = C.  Adds the diagonal (computed from per-string energies) and the
-//     alpha-single x beta-single terms, writes sigma[Ia, Ib] once, and writes the CTA's own
-//     32 x slab tile of C transposed into XT (C^T) through shared memory.
-//   beta pass: X = C^T.  The 32 x slab tile of results goes through shared memory and is added
-//     into sigma[Ia, Ib0..Ib0+31] with 128-byte coalesced read-modify-writes.
-template <typename T, int CPT, bool kAlpha>
-__global__ void __launch_bounds__(kBlkThreads)
+// One kernel, two passes.  A CTA owns kBlkRows consecutive bra strings (rows of X) and a slab of
+// kBlkThreads*VW columns, each thread VW consecutive columns (one 16-byte access when the row
+// length allows it).  Blocks run slab-major so the CTAs in flight gather from one slab of X that
+// stays in L2.  The block's table entries (one contiguous CSR range) are staged in shared memory
+// first, so the gathers X[ket, cols] issue back to back.
+//   alpha pass (kAlpha): X = C.  Adds the diagonal and the alpha-single x beta-single terms and
+//     writes sigma[Ia, Ib] once; the thread's own C[Ia-block, cols] values go out transposed to
+//     C^T as kBlkRows-element contiguous runs.
+//   beta pass: X = C^T.  Each thread adds its kBlkRows x VW results into
+//     sigma[Ia, Ib0 .. Ib0+kBlkRows) (contiguous along Ib) for its columns Ia.
+template <typename T, bool kAlpha, bool kVec>
+__global__ void __launch_bounds__(kBlkThreads, 1)
     sigma_block_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int W = kBlkThreads * VW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int W = kBlkThreads * CPT;
-  T(*tile)[W + 1] = reinterpret_cast<T(*)[W + 1]>(smem_raw);
+  uint32_t *sd_ket = reinterpret_cast<uint32_t *>(smem_raw);
+  T *sd_val = reinterpret_cast<T *>(smem_raw + ((a.max_d * 4 + 15) & ~15u));
+  unsigned char *sp = smem_raw + ((a.max_d * 4 + 15) & ~15u) + a.max_d * sizeof(T);
+  sp = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sp) + 15) & ~(uintptr_t)15);
+  uint32_t *ss_ket = reinterpret_cast<uint32_t *>(sp);
+  int32_t *ss_pair = reinterpret_cast<int32_t *>(sp + a.max_s * 4);
+  double *ss_val = reinterpret_cast<double *>(sp + ((a.max_s * 8 + 15) & ~15u));
+
   const uint32_t nrb = (a.nrows + kBlkRows - 1) / kBlkRows;
   const uint32_t rb = blockIdx.x % nrb, slab = blockIdx.x / nrb;
-  const uint32_t r0 = rb * kBlkRows, c0 = slab * W;
+  const uint32_t r0 = rb * kBlkRows;
   const uint32_t ncols = a.ncols;
   const int L = a.L, L2 = L * L;
   const int nr = (int)min((uint32_t)kBlkRows, a.nrows - r0);
-  uint32_t col[CPT];
-  bool ok[CPT];
-  uint64_t cstr[CPT];
-  double ecol[CPT];
-#pragma unroll
-  for (int k = 0; k < CPT; k++) {
-    col[k] = c0 + threadIdx.x + k * kBlkThreads;
-    ok[k] = col[k] < ncols;
-    cstr[k] = ok[k] ? __ldg(&a.col_str[col[k]]) : 0ull;
-    ecol[k] = (kAlpha && ok[k]) ? __ldg(&a.Eb[col[k]]) : 0.0;
+  const uint32_t cbase = slab * W + threadIdx.x * VW;  // first of this thread's VW columns
+
+  // stage the block's table entries
+  const uint32_t dlo = __ldg(&a.d_off[r0]), dhi = __ldg(&a.d_off[r0 + nr]);
+  const uint32_t slo = __ldg(&a.s_off[r0]), shi = __ldg(&a.s_off[r0 + nr]);
+  for (uint32_t e = dlo + threadIdx.x; e < dhi; e += blockDim.x) {
+    sd_ket[e - dlo] = __ldg(&a.d_ket[e]);
+    sd_val[e - dlo] = val_of<T>(a.d_val, a.d_valf, e);
   }
-  for (int r = 0; r < nr; r++) {
-    const uint32_t row = r0 + r;
-    T acc[CPT];
+  for (uint32_t e = slo + threadIdx.x; e < shi; e += blockDim.x) {
+    ss_ket[e - slo] = __ldg(&a.s_ket[e]);
+    ss_pair[e - slo] = __ldg(&a.s_pair[e]);
+    ss_val[e - slo] = (double)val_of<T>(a.s_val, a.s_valf, e);
+  }
+  __syncthreads();
+
+  bool ok[VW];
+  uint64_t cstr[VW];
 #pragma unroll
-    for (int k = 0; k < CPT; k++) acc[k] = T(0);
-    const uint32_t d0 = __ldg(&a.d_off[row]), d1 = __ldg(&a.d_off[row + 1]);
+  for (int i = 0; i < VW; i++) {
+    ok[i] = cbase + i < ncols;
+    cstr[i] = ok[i] ? __ldg(&a.col_str[cbase + i]) : 0ull;
+  }
+  const bool any = ok[0];
+  const bool full = ok[VW - 1];
+
+  T acc[kBlkRows][VW];
+  T own[kAlpha ? kBlkRows : 1][VW];
+#pragma unroll
+  for (int r = 0; r < kBlkRows; r++) {
+#pragma unroll
+    for (int i = 0; i < VW; i++) {
+      acc[r][i] = T(0);
+      if (kAlpha) own[r][i] = T(0);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kBlkRows; r++) {
+    if (r >= nr || !any) continue;
+    const uint32_t row = r0 + r;
+    const uint32_t d0 = __ldg(&a.d_off[row]) - dlo, d1 = __ldg(&a.d_off[row + 1]) - dlo;
 #pragma unroll 4
     for (uint32_t e = d0; e < d1; e++) {
-      const uint32_t ket = __ldg(&a.d_ket[e]);
-      const T v = val_of<T>(a.d_val, a.d_valf, e);
-      const T *xr = X + (size_t)ket * ncols;
+      const T v = sd_val[e];
+      const T *xr = X + (size_t)sd_ket[e] * ncols + cbase;
+      Vec<T, VW, kVec> x;
+      if (kVec && full) {
+        x.load(xr);
+      } else {
 #pragma unroll
-      for (int k = 0; k < CPT; k++)
-        if (ok[k]) acc[k] += v * __ldg(&xr[col[k]]);
+        for (int i = 0; i < VW; i++) x.v[i] = ok[i] ? __ldg(xr + i) : T(0);
+      }
+#pragma unroll
+      for (int i = 0; i < VW; i++) acc[r][i] += v * x.v[i];
     }
-    const uint32_t s0 = __ldg(&a.s_off[row]), s1 = __ldg(&a.s_off[row + 1]);
+    const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
     for (uint32_t e = s0; e < s1; e++) {
-      const uint32_t ket = __ldg(&a.s_ket[e]);
-      const double v = (double)val_of<T>(a.s_val, a.s_valf, e);
-      const int32_t ps = __ldg(&a.s_pair[e]);
+      const uint32_t ket = ss_ket[e];
+      const double v = ss_val[e];
+      const int32_t ps = ss_pair[e];
       const int pr = (ps > 0 ? ps : -ps) - 1;
       const double sg = ps > 0 ? 1.0 : -1.0;
       const double *vrow = a.vd + (size_t)pr * L;
       const T *xr = X + (size_t)ket * ncols;
 #pragma unroll
-      for (int k = 0; k < CPT; k++) {
-        if (!ok[k]) continue;
-        uint64_t occ = cstr[k];
+      for (int i = 0; i < VW; i++) {
+        if (!ok[i]) continue;
+        const uint32_t c = cbase + i;
+        uint64_t occ = cstr[i];
         double o = 0.0;
         while (occ) {
           o += __ldg(&vrow[lowest_bit(occ)]);
           occ &= occ - 1;
         }
-        double x = (v + sg * o) * (double)__ldg(&xr[col[k]]);
+        double x = (v + sg * o) * (double)__ldg(&xr[c]);
         if (kAlpha && a.do_ab) {
           // this alpha single (ket = Ja, pair pr, sign sg) x every beta single of column Ib
-          for (uint32_t f = __ldg(&a.bs_off[col[k]]); f < __ldg(&a.bs_off[col[k] + 1]); f++) {
+          const uint32_t f1 = __ldg(&a.bs_off[c + 1]);
+          for (uint32_t f = __ldg(&a.bs_off[c]); f < f1; f++) {
             const int32_t pb = __ldg(&a.bs_pair[f]);
             const int rs = (pb > 0 ? pb : -pb) - 1;
             const double g = __ldg(&a.eri[(size_t)pr * L2 + rs]);
@@ -135,43 +206,39 @@ __global__ void __launch_bounds__(kBlkThreads)
             x += (pb > 0 ? g : -g) * cj * sg;
           }
         }
-        acc[k] += (T)x;
+        acc[r][i] += (T)x;
       }
     }
     if (kAlpha) {
-      const double erow = a.core_shift + __ldg(&a.Ea[row]);
-      const double *urow = a.uJ + (size_t)row * L;
+      const size_t idx = (size_t)row * ncols + cbase;
+      Vec<T, VW, kVec> xo;
+      if (kVec && full) {
+        xo.load(X + idx);
+      } else {
 #pragma unroll
-      for (int k = 0; k < CPT; k++) {
-        if (!ok[k]) continue;
-        const size_t idx = (size_t)row * ncols + col[k];
-        const T own = __ldg(&X[idx]);
-        tile[r][threadIdx.x + k * kBlkThreads] = own;
-        // H_ii - shift = I0 + E(Ia) + E(Ib) + sum_{q in Ib} uJ[Ia][q] - shift
-        uint64_t occ = cstr[k];
-        double hd = erow + ecol[k];
-        while (occ) {
-          hd += __ldg(&urow[lowest_bit(occ)]);
-          occ &= occ - 1;
-        }
-        double res = (double)acc[k] + hd * (double)own;
-        if (a.accumulate) res += (double)out[idx];
-        out[idx] = (T)res;
+        for (int i = 0; i < VW; i++) xo.v[i] = ok[i] ? __ldg(X + idx + i) : T(0);
       }
-    } else {
 #pragma unroll
-      for (int k = 0; k < CPT; k++) tile[r][threadIdx.x + k * kBlkThreads] = acc[k];
+      for (int i = 0; i < VW; i++) {
+        own[r][i] = xo.v[i];
+        if (!ok[i]) continue;
+        double res = (double)acc[r][i] + (__ldg(&a.hii[idx + i]) - a.shift) * (double)xo.v[i];
+        if (a.accumulate) res += (double)out[idx + i];
+        out[idx + i] = (T)res;
+      }
     }
   }
-  __syncthreads();
-  // transposed write-out: lane = row within the block, one warp per column
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t ccount = min((uint32_t)W, ncols - c0);
-  for (uint32_t c = warp; c < ccount; c += kBlkThreads / 32) {
-    if (lane >= nr) continue;
-    const size_t o = (size_t)(c0 + c) * a.nrows + r0 + lane;
-    if (kAlpha) XT[o] = tile[lane][c];
-    else out[o] += tile[lane][c];
+  // transposed write-out: column c gets rows r0 .. r0+nr contiguous (index c * nrows + r)
+#pragma unroll
+  for (int i = 0; i < VW; i++) {
+    const size_t o = (size_t)(cbase + i) * a.nrows + r0;
+#pragma unroll
+    for (int r = 0; r < kBlkRows; r++) {
+      if (r < nr && ok[i]) {
+        if (kAlpha) XT[o + r] = own[r][i];
+        else out[o + r] += acc[r][i];
+      }
+    }
   }
 }
 
@@ -213,18 +280,35 @@ int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y) {
   return SBD_TPB_OK;
 }
 
-template <typename T, int CPT, bool kAlpha>
+template <typename T, bool kAlpha>
 int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
-  constexpr int W = kBlkThreads * CPT;
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int W = kBlkThreads * VW;
   const size_t nrb = (ba.nrows + kBlkRows - 1) / kBlkRows, nslab = (ba.ncols + W - 1) / W;
   const size_t blocks = nrb * nslab;
   if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
-  const size_t smem = sizeof(T) * kBlkRows * (W + 1);
-  auto kern = sigma_block_kernel<T, CPT, kAlpha>;
+  const size_t smem = ((ba.max_d * 4 + 15) & ~(size_t)15) + (size_t)ba.max_d * sizeof(T) + 16 +
+                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16;
+  if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
+  // 16-byte column accesses need every row of X to start 16-byte aligned
+  const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
+                   (!kAlpha || (ba.nrows % VW) == 0 || true);
+  auto kern = vec ? sigma_block_kernel<T, kAlpha, true> : sigma_block_kernel<T, kAlpha, false>;
   TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
   TPB_LAUNCHED(h);
   return SBD_TPB_OK;
+}
+
+// Most entries of any kBlkRows-row block of a CSR table (shared-memory staging size).
+uint32_t max_block_entries(const ExTable &t, size_t n) {
+  std::vector<uint32_t> off(n + 1);
+  if (n == 0 || cudaMemcpy(off.data(), t.off, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost) !=
+                    cudaSuccess)
+    return 0;
+  uint32_t mx = 0;
+  for (size_t r = 0; r < n; r += kBlkRows) mx = std::max(mx, off[std::min(n, r + kBlkRows)] - off[r]);
+  return mx;
 }
 
 template <typename T>
@@ -240,7 +324,13 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
     h->ct_bytes = n * sizeof(double);
   }
   T *CT = reinterpret_cast<T *>(h->d_ct);
-  constexpr int CPT = sizeof(T) == 4 ? 4 : 2;
+  if (h->blk_for != (const void *)h->ta_d.ket) {
+    h->blk_max[0] = max_block_entries(h->ta_d, na);
+    h->blk_max[1] = max_block_entries(h->ta_s, na);
+    h->blk_max[2] = max_block_entries(h->tb_d, nb);
+    h->blk_max[3] = max_block_entries(h->tb_s, nb);
+    h->blk_for = h->ta_d.ket;
+  }
 
   BlockArgs ba{};
   ba.s_off = h->ta_s.off;
@@ -257,10 +347,10 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   ba.L = h->L;
   ba.nrows = na;
   ba.ncols = nb;
-  ba.core_shift = h->I0 - shift;
-  ba.Ea = h->d_Ea;
-  ba.Eb = h->d_Eb;
-  ba.uJ = h->d_uJ;
+  ba.max_d = h->blk_max[0];
+  ba.max_s = h->blk_max[1];
+  ba.hii = h->d_hii;
+  ba.shift = shift;
   ba.accumulate = accumulate;
   ba.do_ab = dense_ab ? 0 : 1;
   ba.bs_off = h->tb_s.off;
@@ -268,7 +358,7 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   ba.bs_pair = h->pb.s_pair;
   ba.eri = h->d_eri;
   TPB_CUDA(cudaEventRecord(h->ev0, h->stream));
-  TPB_CHECK((launch_block<T, CPT, true>(h, ba, C, sigma, CT)));
+  TPB_CHECK((launch_block<T, true>(h, ba, C, sigma, CT)));
   TPB_CUDA(cudaEventRecord(h->ev_k[0], h->stream));
 
   BlockArgs bb{};
@@ -286,7 +376,9 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   bb.L = h->L;
   bb.nrows = nb;
   bb.ncols = na;
-  TPB_CHECK((launch_block<T, CPT, false>(h, bb, CT, sigma, nullptr)));
+  bb.max_d = h->blk_max[2];
+  bb.max_s = h->blk_max[3];
+  TPB_CHECK((launch_block<T, false>(h, bb, CT, sigma, nullptr)));
   TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
   h->sigma_kernels = 2;
   if (dense_ab) TPB_CHECK(ab_dense_apply<T>(h, C, sigma));

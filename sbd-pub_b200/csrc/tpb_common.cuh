@@ -153,6 +153,8 @@ struct sbd_tpb_handle {
   double *d_tmp64 = nullptr;     // one N-vector FP64 (sign conversion staging)
   double *d_tmp64b = nullptr;
   float *d_tmp32 = nullptr, *d_tmp32b = nullptr;
+  uint32_t blk_max[4] = {0, 0, 0, 0};  // per-block table entries (alpha d/s, beta d/s)
+  const void *blk_for = nullptr;        // tables blk_max was computed for
   void *d_ct = nullptr;          // C^T staging of the beta pass of sigma
   size_t ct_bytes = 0;
   void *d_ab_work = nullptr;     // dense alpha-beta intermediates
