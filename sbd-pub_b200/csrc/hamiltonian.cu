@@ -55,6 +55,13 @@ __global__ void diag_kernel(const uint64_t *__restrict__ astr, const uint64_t *_
   }
 }
 
+__global__ void diag32_kernel(const double *__restrict__ hii, size_t n, double h00,
+                              float *__restrict__ hii32) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    hii32[i] = (float)(hii[i] - h00);
+}
+
 // Values of the sigma program, aligned entry by entry with the excitation tables.
 __global__ void single_values_kernel(const uint64_t *__restrict__ str, uint32_t n, int L,
                                      const uint32_t *__restrict__ off,
@@ -153,6 +160,7 @@ void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->d_Eb);
   free_dev(h->d_uJ);
   free_dev(h->d_hii);
+  free_dev(h->d_hii32);
   for (ExTable *t : {&h->ta_s, &h->ta_d, &h->tb_s, &h->tb_d}) {
     free_dev(t->off);
     free_dev(t->ket);
@@ -270,6 +278,12 @@ int compute_diagonal(sbd_tpb_handle *h) {
   diag_kernel<<<grid, 256, 0, h->stream>>>(h->d_astr, h->d_bstr, h->d_Ea, h->d_Eb, h->d_uJ, h->L,
                                           (uint32_t)h->astr.size(), (uint32_t)h->bstr.size(),
                                           h->I0, h->d_hii);
+  TPB_LAUNCHED(h);
+  TPB_CUDA(cudaMemcpyAsync(&h->h00, h->d_hii, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TPB_CUDA(cudaStreamSynchronize(h->stream));
+  free_dev(h->d_hii32);
+  TPB_CUDA(cudaMalloc(&h->d_hii32, sizeof(float) * n));
+  diag32_kernel<<<grid, 256, 0, h->stream>>>(h->d_hii, n, h->h00, h->d_hii32);
   TPB_LAUNCHED(h);
   return SBD_TPB_OK;
 }

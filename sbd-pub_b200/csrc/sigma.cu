@@ -51,11 +51,6 @@ struct Vec<float, 4, kVec> {
       for (int i = 0; i < 4; i++) v[i] = __ldg(p + i);
     }
   }
-  // read-once data: evict-first, so the gathered slab keeps its place in L2
-  __device__ __forceinline__ void load_stream(const float *p) {
-    const float4 f = __ldcs(reinterpret_cast<const float4 *>(p));
-    v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
-  }
 };
 template <bool kVec>
 struct Vec<double, 2, kVec> {
@@ -68,10 +63,6 @@ struct Vec<double, 2, kVec> {
       v[0] = __ldg(p);
       v[1] = __ldg(p + 1);
     }
-  }
-  __device__ __forceinline__ void load_stream(const double *p) {
-    const double2 f = __ldcs(reinterpret_cast<const double2 *>(p));
-    v[0] = f.x, v[1] = f.y;
   }
 };
 
@@ -91,7 +82,9 @@ struct BlockArgs {
   uint32_t max_d, max_s;    // most doubles / singles entries of any kBlkRows-row block
   // alpha pass only: diagonal (H_ii = I0 + E(Ia) + E(Ib) + sum_{q in Ib} uJ[Ia][q]) and the
   // alpha-single x beta-single terms
-  double core_shift;  // I0 - shift
+  double core_shift;     // FP64 pass: shift; FP32 pass: H_00 - shift
+  const double *hii;     // FP64 diagonal
+  const float *hii32;    // H_ii - H_00 in FP32
   const double *Ea, *Eb, *uJ;
   int accumulate;
   int do_ab;
@@ -123,7 +116,6 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
   uint32_t *ss_ket = reinterpret_cast<uint32_t *>(sp);
   int32_t *ss_pair = reinterpret_cast<int32_t *>(sp + a.max_s * 4);
   double *ss_val = reinterpret_cast<double *>(sp + ((a.max_s * 8 + 15) & ~15u));
-  double *s_uj = ss_val + a.max_s;  // [kBlkRows][L] rows of uJ (alpha pass)
 
   const uint32_t nrb = (a.nrows + kBlkRows - 1) / kBlkRows;
   const uint32_t rb = blockIdx.x % nrb, slab = blockIdx.x / nrb;
@@ -145,18 +137,14 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
     ss_pair[e - slo] = __ldg(&a.s_pair[e]);
     ss_val[e - slo] = (double)val_of<T>(a.s_val, a.s_valf, e);
   }
-  if (kAlpha)
-    for (int t = threadIdx.x; t < nr * L; t += blockDim.x) s_uj[t] = __ldg(&a.uJ[(size_t)r0 * L + t]);
   __syncthreads();
 
   bool ok[VW];
   uint64_t cstr[VW];
-  double ecol[VW];
 #pragma unroll
   for (int i = 0; i < VW; i++) {
     ok[i] = cbase + i < ncols;
     cstr[i] = ok[i] ? __ldg(&a.col_str[cbase + i]) : 0ull;
-    ecol[i] = (kAlpha && ok[i]) ? __ldg(&a.Eb[cbase + i]) : 0.0;
   }
   const bool any = ok[0];
   const bool full = ok[VW - 1];
@@ -176,7 +164,7 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
     if (r >= nr || !any) continue;
     const uint32_t row = r0 + r;
     const uint32_t d0 = __ldg(&a.d_off[row]) - dlo, d1 = __ldg(&a.d_off[row + 1]) - dlo;
-#pragma unroll 8
+#pragma unroll 4
     for (uint32_t e = d0; e < d1; e++) {
       const T v = sd_val[e];
       const T *xr = X + (size_t)sd_ket[e] * ncols + cbase;
@@ -228,26 +216,22 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
       const size_t idx = (size_t)row * ncols + cbase;
       Vec<T, VW, kVec> xo;
       if (kVec && full) {
-        xo.load_stream(X + idx);
+        xo.load(X + idx);
       } else {
 #pragma unroll
-        for (int i = 0; i < VW; i++) xo.v[i] = ok[i] ? __ldcs(X + idx + i) : T(0);
+        for (int i = 0; i < VW; i++) xo.v[i] = ok[i] ? __ldg(X + idx + i) : T(0);
       }
-      const double erow = a.core_shift + __ldg(&a.Ea[row]);
-      const double *urow = s_uj + r * L;
 #pragma unroll
       for (int i = 0; i < VW; i++) {
         own[r][i] = xo.v[i];
         if (!ok[i]) continue;
-        double hd = erow + ecol[i];
-        uint64_t occ = cstr[i];
-        while (occ) {
-          hd += urow[lowest_bit(occ)];
-          occ &= occ - 1;
-        }
+        // H_ii - shift: FP64 diagonal for the FP64 pass, (H_ii - H_00) in FP32 plus the FP64
+        // constant H_00 - shift for the FP32 pass
+        const double hd = sizeof(T) == 8 ? __ldg(&a.hii[idx + i]) - a.core_shift
+                                         : (double)__ldg(&a.hii32[idx + i]) + a.core_shift;
         double res = (double)acc[r][i] + hd * (double)xo.v[i];
         if (a.accumulate) res += (double)out[idx + i];
-        __stcs(out + idx + i, (T)res);
+        out[idx + i] = (T)res;
       }
     }
   }
@@ -258,8 +242,8 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
 #pragma unroll
     for (int r = 0; r < kBlkRows; r++) {
       if (r < nr && ok[i]) {
-        if (kAlpha) __stcs(XT + o + r, own[r][i]);
-        else __stcs(out + o + r, __ldcs(out + o + r) + acc[r][i]);
+        if (kAlpha) XT[o + r] = own[r][i];
+        else out[o + r] += acc[r][i];
       }
     }
   }
@@ -311,8 +295,7 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   const size_t blocks = nrb * nslab;
   if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
   const size_t smem = ((ba.max_d * 4 + 15) & ~(size_t)15) + (size_t)ba.max_d * sizeof(T) + 16 +
-                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16 +
-                      (kAlpha ? (size_t)kBlkRows * ba.L * sizeof(double) : 0);
+                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16;
   if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
   // 16-byte column accesses need every row of X to start 16-byte aligned
   const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
@@ -373,10 +356,9 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   ba.ncols = nb;
   ba.max_d = h->blk_max[0];
   ba.max_s = h->blk_max[1];
-  ba.core_shift = h->I0 - shift;
-  ba.Ea = h->d_Ea;
-  ba.Eb = h->d_Eb;
-  ba.uJ = h->d_uJ;
+  ba.hii = h->d_hii;
+  ba.hii32 = h->d_hii32;
+  ba.core_shift = sizeof(T) == 8 ? shift : h->h00 - shift;
   ba.accumulate = accumulate;
   ba.do_ab = dense_ab ? 0 : 1;
   ba.bs_off = h->tb_s.off;

@@ -143,6 +143,8 @@ struct sbd_tpb_handle {
   double *d_Ea = nullptr, *d_Eb = nullptr;  // same-spin string energies
   double *d_uJ = nullptr;    // [na][L]: sum_{p in Ia} (pp|qq)
   double *d_hii = nullptr;   // [na*nb] FP64 diagonal
+  float *d_hii32 = nullptr;  // [na*nb] H_ii - H_00 in FP32 (FP32 sigma)
+  double h00 = 0.0;          // H_00
   sbdtpb::ExTable ta_s, ta_d, tb_s, tb_d;
   sbdtpb::SigmaProg pa, pb;
   sbdtpb::ABDense ab;
