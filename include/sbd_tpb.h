@@ -150,6 +150,22 @@ SBD_TPB_API int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigm
 SBD_TPB_API int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
                                      int accumulate, int convention);
 
+/* Size of the fixed device scratch of sbd_tpb_sigma_noalloc (16 MiB). */
+#define SBD_TPB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+
+/* sigma (+)= H*C on device vectors in the separated convention (as sbd_tpb_sigma_device with
+ * convention 1) that allocates no device memory.  No counterpart in the reference: it serves
+ * callers that cannot have a library call cudaMalloc under them -- a code that has already
+ * reserved the card's memory through its own pool, or work issued inside stream capture.  The
+ * C^T staging lives in a static device array of SBD_TPB_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit; ndet * element size beyond it is rejected with
+ * SBD_TPB_ERR_INVALID.  All calls on a device share that array (nothing in it must start at
+ * zero), so calls whose kernels overlap on the GPU race: serialise them.  The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress) and reads the table offsets back
+ * once: make it before any stream capture.  The alpha-beta terms always use the direct loop. */
+SBD_TPB_API int sbd_tpb_sigma_noalloc(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
+                                      int accumulate);
+
 /* Davidson (tpb/davidson.h:667-930; basic/davidson_thrust.h:85-373) on the handle's problem,
  * from W (host, [na*nb], reference convention; NULL = HF start).  Writes the energy etc. into
  * result (ci_vector/density/RDM fields as in sbd_tpb_diag). */

@@ -394,6 +394,74 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   return SBD_TPB_OK;
 }
 
+// Same two passes with a caller-provided C^T buffer and the alpha-beta terms always evaluated by
+// the direct loop of the alpha pass: needs no device memory beyond C, sigma and CT.
+template <typename T>
+int sigma_sep_given_ct(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, T *CT) {
+  const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
+  if (h->blk_for != (const void *)h->ta_d.ket) {
+    h->blk_max[0] = max_block_entries(h->ta_d, na);
+    h->blk_max[1] = max_block_entries(h->ta_s, na);
+    h->blk_max[2] = max_block_entries(h->tb_d, nb);
+    h->blk_max[3] = max_block_entries(h->tb_s, nb);
+    h->blk_for = h->ta_d.ket;
+  }
+  BlockArgs ba{};
+  ba.s_off = h->ta_s.off;
+  ba.s_ket = h->ta_s.ket;
+  ba.s_val = h->pa.s_val;
+  ba.s_valf = h->pa.s_valf;
+  ba.s_pair = h->pa.s_pair;
+  ba.d_off = h->ta_d.off;
+  ba.d_ket = h->ta_d.ket;
+  ba.d_val = h->pa.d_val;
+  ba.d_valf = h->pa.d_valf;
+  ba.col_str = h->d_bstr;
+  ba.vd = h->d_vd;
+  ba.L = h->L;
+  ba.nrows = na;
+  ba.ncols = nb;
+  ba.max_d = h->blk_max[0];
+  ba.max_s = h->blk_max[1];
+  ba.hii = h->d_hii;
+  ba.hii32 = h->d_hii32;
+  ba.core_shift = sizeof(T) == 8 ? 0.0 : h->h00;
+  ba.accumulate = accumulate;
+  ba.do_ab = 1;
+  ba.bs_off = h->tb_s.off;
+  ba.bs_ket = h->tb_s.ket;
+  ba.bs_pair = h->pb.s_pair;
+  ba.eri = h->d_eri;
+  TPB_CUDA(cudaEventRecord(h->ev0, h->stream));
+  TPB_CHECK((launch_block<T, true>(h, ba, C, sigma, CT)));
+  TPB_CUDA(cudaEventRecord(h->ev_k[0], h->stream));
+  BlockArgs bb{};
+  bb.s_off = h->tb_s.off;
+  bb.s_ket = h->tb_s.ket;
+  bb.s_val = h->pb.s_val;
+  bb.s_valf = h->pb.s_valf;
+  bb.s_pair = h->pb.s_pair;
+  bb.d_off = h->tb_d.off;
+  bb.d_ket = h->tb_d.ket;
+  bb.d_val = h->pb.d_val;
+  bb.d_valf = h->pb.d_valf;
+  bb.col_str = h->d_astr;
+  bb.vd = h->d_vd;
+  bb.L = h->L;
+  bb.nrows = nb;
+  bb.ncols = na;
+  bb.max_d = h->blk_max[2];
+  bb.max_s = h->blk_max[3];
+  TPB_CHECK((launch_block<T, false>(h, bb, CT, sigma, nullptr)));
+  TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
+  h->sigma_kernels = 2;
+  TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
+  return SBD_TPB_OK;
+}
+
+template int sigma_sep_given_ct<double>(sbd_tpb_handle *, const double *, double *, int, double *);
+template int sigma_sep_given_ct<float>(sbd_tpb_handle *, const float *, float *, int, float *);
+
 template <typename T>
 int sigma_sep(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate) {
   return sigma_sep_shift<T>(h, C, sigma, accumulate, 0.0);

@@ -181,6 +181,9 @@ int sigma_sep(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate);
 // sigma (+)= (H - shift) C
 template <typename T>
 int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, double shift);
+// sigma (+)= H C with a caller-provided C^T buffer of ndet elements; no device allocation
+template <typename T>
+int sigma_sep_given_ct(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, T *CT);
 int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y);
 int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y);
 // ab_dense.cu: alpha-beta term as gather -> dense (pq|rs) contraction -> scatter

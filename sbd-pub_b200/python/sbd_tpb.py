@@ -37,7 +37,7 @@ EXPORTED = [
     "sbd_tpb_default_params", "sbd_tpb_diag", "sbd_tpb_last_error", "sbd_tpb_create",
     "sbd_tpb_destroy", "sbd_tpb_set_hamiltonian", "sbd_tpb_set_strings", "sbd_tpb_build_tables",
     "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
-    "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
+    "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_sigma_noalloc", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
     "sbd_tpb_last_sigma_ms", "sbd_tpb_last_sigma_kernels", "sbd_tpb_kernel_launches",
 ]
 
@@ -102,6 +102,7 @@ def lib():
     L.sbd_tpb_sigma.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.sbd_tpb_sigma_f32.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.sbd_tpb_sigma_device.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int]
+    L.sbd_tpb_sigma_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.sbd_tpb_davidson.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
     L.sbd_tpb_rdm.argtypes = [vp, vp, vp, vp, C.c_int]
     L.sbd_tpb_stream.restype = vp
@@ -227,6 +228,13 @@ class Handle:
         dt = 1 if str(x.dtype) == "torch.float32" else 0
         _check(lib().sbd_tpb_sigma_device(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate),
                                           1 if separated else 0))
+        return y
+
+    def sigma_noalloc(self, x, y, accumulate=False):
+        """sigma into caller-owned torch CUDA tensors without any device allocation by the
+        library (separated convention, fixed 16 MiB scratch; see sbd_tpb_sigma_noalloc)."""
+        dt = 1 if str(x.dtype) == "torch.float32" else 0
+        _check(lib().sbd_tpb_sigma_noalloc(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate)))
         return y
 
     def last_sigma_ms(self) -> float:

@@ -26,7 +26,7 @@ def test_library_exports_header():
 
 def test_binding_declares_every_symbol():
     import sbd_tpb
-    assert set(declared_symbols()) <= set(sbd_tpb.EXPORTED) | {"sbd_tpb_sigma_noalloc"}
+    assert set(declared_symbols()) <= set(sbd_tpb.EXPORTED)
 
 
 def test_no_device_returns_status():
