@@ -12,8 +12,10 @@
 // double.  The mixed path stores C/HC/W/t in FP32, computes sigma of (H - s) with s = H_00 so the
 // FP32 entries carry residual-sized values, keeps all dot products and the Rayleigh-Ritz in FP64,
 // and finishes with one FP64 sigma on the converged vector for the reported energy and residual.
-// Both orthogonalise with two rounds of classical Gram-Schmidt (as stable as the reference's
-// modified Gram-Schmidt, tpb/davidson.h:871-879, with two fused passes instead of k+1).
+// Both orthogonalise with classical Gram-Schmidt, repeated once when the first round cancels more
+// than half of |t|^2 (as stable as the reference's modified Gram-Schmidt, tpb/davidson.h:871-879,
+// with one or two fused passes instead of k+1).  The converged vector stays in HBM for the final
+// sigma and the RDMs; it crosses to the host only when the caller asks for it.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -91,86 +93,94 @@ struct DevVec {
 
 template <typename T>
 int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, double shift,
-              int cgs_rounds, sbd_tpb_result *res, std::vector<double> &Wout_sep,
-              double *resid_out, int *nsigma_out, int *converged_out) {
+              double *dWout, double *resid_out, int *nsigma_out, int *converged_out) {
   const size_t n = h->ndet();
   const int nb = prm->max_nb;
   const int max_it = prm->max_it;
-  std::vector<DevVec<T>> C(nb), HC(nb);
-  DevVec<T> Wv, tv;
+  std::vector<DevVec<T>> S(nb), HS(nb);
+  DevVec<T> Wv;
   for (int k = 0; k < nb; k++) {
-    TPB_CUDA(cudaMalloc(&C[k].p, sizeof(T) * n));
-    TPB_CUDA(cudaMalloc(&HC[k].p, sizeof(T) * n));
+    TPB_CUDA(cudaMalloc(&S[k].p, sizeof(T) * n));
+    TPB_CUDA(cudaMalloc(&HS[k].p, sizeof(T) * n));
   }
   TPB_CUDA(cudaMalloc(&Wv.p, sizeof(T) * n));
-  TPB_CUDA(cudaMalloc(&tv.p, sizeof(T) * n));
 
-  // initial vector (separated convention)
+  // Subspace vectors are stored unnormalised: the basis vector is C_k = f_k S_k and
+  // H C_k = f_k sigma(S_k), so normalising costs no pass over the vector.
+  std::vector<double> f(nb, 1.0);
+
+  // initial vector (separated convention), staged through dWout
   {
-    DevVec<double> w64;
-    TPB_CUDA(cudaMalloc(&w64.p, sizeof(double) * n));
     if (W0) {
-      TPB_CUDA(cudaMemcpyAsync(w64.p, W0, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-      TPB_CHECK(reorder_sign_apply_f64(h, w64.p, w64.p));
+      TPB_CUDA(cudaMemcpyAsync(dWout, W0, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+      TPB_CHECK(reorder_sign_apply_f64(h, dWout, dWout));
     } else {
       // --init 0: the first determinant, i.e. the HF string when it is the smallest
       // (tpb/davidson.h:134-137)
-      TPB_CUDA(cudaMemsetAsync(w64.p, 0, sizeof(double) * n, h->stream));
+      TPB_CUDA(cudaMemsetAsync(dWout, 0, sizeof(double) * n, h->stream));
       const double one = 1.0;
-      TPB_CUDA(cudaMemcpyAsync(w64.p, &one, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      TPB_CUDA(cudaMemcpyAsync(dWout, &one, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     }
     if (std::is_same<T, double>::value) {
-      TPB_CUDA(cudaMemcpyAsync(C[0].p, w64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+      TPB_CUDA(cudaMemcpyAsync(S[0].p, dWout, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     } else {
-      TPB_CHECK((convert_vec<double, T>(h, w64.p, C[0].p, n)));
+      TPB_CHECK((convert_vec<double, T>(h, dWout, S[0].p, n)));
     }
     double nrm = 0.0;
-    const T *cp[1] = {C[0].p};
-    TPB_CHECK(multi_dot<T>(h, cp, 1, C[0].p, n, &nrm));
+    const T *cp[1] = {S[0].p};
+    TPB_CHECK(multi_dot<T>(h, cp, 1, S[0].p, n, &nrm));
     if (!(nrm > 0.0)) return fail(SBD_TPB_ERR_INVALID, "initial vector is zero");
-    TPB_CHECK(scale_vec<T>(h, C[0].p, 1.0 / std::sqrt(nrm), n));
+    f[0] = 1.0 / std::sqrt(nrm);
   }
 
   std::vector<double> Hs((size_t)nb * nb, 0.0), E, U;
-  std::vector<double> out(kMaxVec + 2);
+  std::vector<double> out(kMaxVec + 2), dots(kMaxVec + 2);
   std::vector<double> step_times;
   double norm_R = 0.0, ww = 1.0;
-  int nsigma = 0;
-  bool converged = false, stop = false;
+  int nsigma = 0, m_last = 0;
+  bool converged = false, stop = false, w_current = false;
+  ResidualArgs<T> ra;
   const auto t_start = std::chrono::steady_clock::now();
 
   for (int it = 0; it < max_it && !stop; it++) {
     if (it > 0) {
-      // restart from the normalised Ritz vector (tpb/davidson.h:918-922)
-      TPB_CUDA(cudaMemcpyAsync(C[0].p, Wv.p, sizeof(T) * n, cudaMemcpyDeviceToDevice, h->stream));
-      TPB_CHECK(scale_vec<T>(h, C[0].p, 1.0 / std::sqrt(ww), n));
+      // restart from the normalised Ritz vector (tpb/davidson.h:918-922): W becomes S_0
+      std::swap(S[0].p, Wv.p);
+      f[0] = 1.0 / std::sqrt(ww);
+      w_current = false;
     }
     for (int ib = 0; ib < nb; ib++) {
       const auto s0 = std::chrono::steady_clock::now();
-      TPB_CHECK(sigma_sep_shift<T>(h, C[ib].p, HC[ib].p, 0, shift));
+      TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
       nsigma++;
       std::vector<const T *> cp(ib + 1);
-      for (int k = 0; k <= ib; k++) cp[k] = C[k].p;
-      TPB_CHECK(multi_dot<T>(h, cp.data(), ib + 1, HC[ib].p, n, out.data()));
+      for (int k = 0; k <= ib; k++) cp[k] = S[k].p;
+      TPB_CHECK(multi_dot<T>(h, cp.data(), ib + 1, HS[ib].p, n, out.data()));
       for (int k = 0; k <= ib; k++) {
-        Hs[k + (size_t)nb * ib] = out[k];
-        Hs[ib + (size_t)nb * k] = out[k];
+        const double v = f[k] * f[ib] * out[k];
+        Hs[k + (size_t)nb * ib] = v;
+        Hs[ib + (size_t)nb * k] = v;
       }
       jacobi_eigen(ib + 1, Hs.data(), nb, E, U);
-      ResidualArgs<T> ra;
       for (int k = 0; k < kMaxVec; k++) {
-        ra.C.p[k] = k <= ib ? C[k].p : nullptr;
-        ra.HC.p[k] = k <= ib ? HC[k].p : nullptr;
+        ra.C.p[k] = k <= ib ? S[k].p : nullptr;
+        ra.HC.p[k] = k <= ib ? HS[k].p : nullptr;
       }
-      for (int k = 0; k < kMaxSub; k++) ra.u[k] = k <= ib ? U[k] : 0.0;
+      for (int k = 0; k < kMaxSub; k++) ra.u[k] = k <= ib ? U[k] * f[k] : 0.0;
       ra.m = ib + 1;
       ra.e_shifted = E[0];
       ra.e0 = E[0] + shift;
       ra.hii = h->d_hii;
-      ra.W = Wv.p;
-      T *tnext = (ib < nb - 1) ? C[ib + 1].p : tv.p;
+      ra.hii32 = nullptr;
+      // W is needed for the restart after the last step of a cycle; otherwise it is formed
+      // only once, when the loop stops.  The last step of a cycle needs no correction.
+      const bool last = ib == nb - 1;
+      ra.W = last ? Wv.p : nullptr;
+      T *tnext = last ? nullptr : S[ib + 1].p;
       ra.t = tnext;
       TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+      w_current = last;
+      m_last = ib + 1;
       ww = out[0];
       norm_R = std::sqrt(out[1] / ww);
       if (prm->verbose) {
@@ -184,22 +194,27 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         stop = true;
         break;
       }
-      if (ib < nb - 1) {
-        std::vector<double> olap(out.begin() + 2, out.begin() + 2 + ib + 1);
-        double tt = 0.0;
-        for (int round = 0; round < cgs_rounds; round++) {
-          const bool more = round + 1 < cgs_rounds;
-          TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, olap.data(), tnext, n, more ? 1 : 0,
-                                  out.data()));
-          tt = out[0];
-          if (more) olap.assign(out.begin() + 1, out.begin() + 1 + ib + 1);
+      if (!last) {
+        // classical Gram-Schmidt against C_0..C_ib: t -= sum_k (C_k.t) C_k = sum_k f_k^2 (S_k.t) S_k.
+        // A second round runs only when the first cancelled more than half of |t|^2 ("twice is
+        // enough": after a round that keeps |t|^2 >= 1/2 of its input, t is orthogonal to the
+        // subspace to working precision).
+        const double t0 = out[2 + ib + 1];
+        std::vector<double> o(ib + 1);
+        for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * out[2 + k];
+        TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 1, dots.data()));
+        double tt = dots[0];
+        if (tt < 0.5 * t0) {
+          for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * dots[1 + k];
+          TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 0, dots.data()));
+          tt = dots[0];
         }
         if (!(tt > 0.0)) {
           // the correction lies in the subspace: nothing left to add
           stop = true;
           break;
         }
-        TPB_CHECK(scale_vec<T>(h, tnext, 1.0 / std::sqrt(tt), n));
+        f[ib + 1] = 1.0 / std::sqrt(tt);
       }
       // max_time guard (tpb/davidson.h:887-913): stop when the next step would overrun
       TPB_CUDA(cudaStreamSynchronize(h->stream));
@@ -216,28 +231,27 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       }
     }
   }
-  // W = Ritz vector of the last step, normalised, promoted to FP64
-  Wout_sep.resize(n);
-  {
-    DevVec<double> w64;
-    TPB_CUDA(cudaMalloc(&w64.p, sizeof(double) * n));
-    if (std::is_same<T, double>::value) {
-      TPB_CUDA(cudaMemcpyAsync(w64.p, Wv.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-    } else {
-      TPB_CHECK((convert_vec<T, double>(h, Wv.p, w64.p, n)));
-    }
-    double nrm = 0.0;
-    const double *wp[1] = {w64.p};
-    TPB_CHECK(multi_dot<double>(h, wp, 1, w64.p, n, &nrm));
-    TPB_CHECK(scale_vec<double>(h, w64.p, 1.0 / std::sqrt(nrm), n));
-    TPB_CUDA(cudaMemcpyAsync(Wout_sep.data(), w64.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                             h->stream));
-    TPB_CUDA(cudaStreamSynchronize(h->stream));
+  if (!w_current) {
+    // form W = sum_k u_k S_k of the last step (no correction)
+    ra.W = Wv.p;
+    ra.t = nullptr;
+    ra.m = m_last;
+    TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+    ww = out[0];
   }
+  // W normalised and promoted to FP64 into dWout
+  if (std::is_same<T, double>::value) {
+    TPB_CUDA(cudaMemcpyAsync(dWout, Wv.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+  } else {
+    TPB_CHECK((convert_vec<T, double>(h, Wv.p, dWout, n)));
+  }
+  double nrm = 0.0;
+  const double *wp[1] = {dWout};
+  TPB_CHECK(multi_dot<double>(h, wp, 1, dWout, n, &nrm));
+  TPB_CHECK(scale_vec<double>(h, dWout, 1.0 / std::sqrt(nrm), n));
   *resid_out = norm_R;
   *nsigma_out = nsigma;
   *converged_out = converged ? 1 : 0;
-  (void)res;
   return SBD_TPB_OK;
 }
 
@@ -251,53 +265,34 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   if (p->max_it < 1) return fail(SBD_TPB_ERR_INVALID, "davidson: --iteration must be >= 1");
   const size_t n = h->ndet();
   const auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> Wsep;
   double resid = 0.0;
   int nsig = 0, conv = 0;
+  DevVec<double> dW, dHW;
+  TPB_CUDA(cudaMalloc(&dW.p, sizeof(double) * n));
   if (p->precision == SBD_TPB_MIXED) {
     double h00 = 0.0;
     TPB_CUDA(cudaMemcpy(&h00, h->d_hii, sizeof(double), cudaMemcpyDeviceToHost));
-    TPB_CHECK(run_typed<float>(h, p, W0, h00, 2, res, Wsep, &resid, &nsig, &conv));
+    TPB_CHECK(run_typed<float>(h, p, W0, h00, dW.p, &resid, &nsig, &conv));
   } else {
-    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, 2, res, Wsep, &resid, &nsig, &conv));
+    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, dW.p, &resid, &nsig, &conv));
   }
   // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
-  double *dW = nullptr, *dHW = nullptr;
-  TPB_CUDA(cudaMalloc(&dW, sizeof(double) * n));
-  TPB_CUDA(cudaMalloc(&dHW, sizeof(double) * n));
-  int rc = SBD_TPB_OK;
+  TPB_CUDA(cudaMalloc(&dHW.p, sizeof(double) * n));
   double E = 0.0, rr = 0.0;
-  do {
-    if (cudaMemcpyAsync(dW, Wsep.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream) !=
-        cudaSuccess) {
-      rc = fail(SBD_TPB_ERR_CUDA, "davidson: upload of W failed");
-      break;
-    }
-    if ((rc = sigma_sep<double>(h, dW, dHW, 0)) != SBD_TPB_OK) break;
-    const double *wp[1] = {dW};
-    if ((rc = multi_dot<double>(h, wp, 1, dHW, n, &E)) != SBD_TPB_OK) break;
-    if ((rc = axpby<double>(h, dW, dHW, -E, 1.0, n)) != SBD_TPB_OK) break;
-    const double *hp[1] = {dHW};
-    if ((rc = multi_dot<double>(h, hp, 1, dHW, n, &rr)) != SBD_TPB_OK) break;
-    if (res->ci_vector) {
-      if ((rc = reorder_sign_apply_f64(h, dW, dHW)) != SBD_TPB_OK) break;
-      if (cudaMemcpyAsync(res->ci_vector, dHW, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                          h->stream) != cudaSuccess) {
-        rc = fail(SBD_TPB_ERR_CUDA, "davidson: download of W failed");
-        break;
-      }
-    }
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
-      rc = fail(SBD_TPB_ERR_CUDA, "davidson: stream failed");
-      break;
-    }
-    if (res->density || res->one_rdm || res->two_rdm) {
-      if ((rc = rdm_sep(h, dW, res->one_rdm, res->two_rdm, res->density)) != SBD_TPB_OK) break;
-    }
-  } while (0);
-  cudaFree(dW);
-  cudaFree(dHW);
-  TPB_CHECK(rc);
+  TPB_CHECK(sigma_sep<double>(h, dW.p, dHW.p, 0));
+  const double *wp[1] = {dW.p};
+  TPB_CHECK(multi_dot<double>(h, wp, 1, dHW.p, n, &E));
+  TPB_CHECK(axpby<double>(h, dW.p, dHW.p, -E, 1.0, n));
+  const double *hp[1] = {dHW.p};
+  TPB_CHECK(multi_dot<double>(h, hp, 1, dHW.p, n, &rr));
+  if (res->ci_vector) {
+    TPB_CHECK(reorder_sign_apply_f64(h, dW.p, dHW.p));
+    TPB_CUDA(cudaMemcpyAsync(res->ci_vector, dHW.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                             h->stream));
+  }
+  TPB_CUDA(cudaStreamSynchronize(h->stream));
+  if (res->density || res->one_rdm || res->two_rdm)
+    TPB_CHECK(rdm_sep(h, dW.p, res->one_rdm, res->two_rdm, res->density));
   res->energy = E;
   res->residual = (p->precision == SBD_TPB_MIXED) ? std::sqrt(rr) : resid;
   res->iterations = nsig;

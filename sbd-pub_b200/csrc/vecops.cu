@@ -66,8 +66,8 @@ __global__ void reduce_partials_kernel(const double *__restrict__ partials, int 
   if (threadIdx.x == 0) out[blockIdx.x] = s[0];
 }
 
-// W = sum_k u_k C_k ; r = E' W - sum_k u_k HC_k ; t = r / (E0 - H_ii) (regularised as
-// tpb/davidson.h:861-868) ; partials: [0] = W.W, [1] = r.r, [2+k] = C_k . t
+// W = sum_k u_k S_k ; r = E' W - sum_k u_k sigma(S_k) ; t = r / (E0 - H_ii) (regularised as
+// tpb/davidson.h:861-868) ; partials: [0] = W.W, [1] = r.r, [2+k] = S_k . t, [2+m] = t.t
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
     residual_kernel(ResidualArgs<T> a, size_t n, double *partials) {
@@ -88,18 +88,22 @@ __global__ void __launch_bounds__(kVecThreads)
       }
     }
     const double r = a.e_shifted * w - hc;
-    const double d = a.e0 - a.hii[i];
-    const double t = (fabs(d) > 1.0e-12) ? r / d : r / (d - 1.0e-12);
     if (a.W) a.W[i] = (T)w;
-    const T tt = (T)t;
-    a.t[i] = tt;
     acc[0] += w * w;
     acc[1] += r * r;
+    if (a.t) {
+      const double hd = a.hii32 ? (double)a.hii32[i] : a.hii[i];
+      const double d = a.e0 - hd;
+      const double t = (fabs(d) > 1.0e-12) ? r / d : r / (d - 1.0e-12);
+      const T tt = (T)t;
+      a.t[i] = tt;
 #pragma unroll
-    for (int k = 0; k < kMaxSub; k++)
-      if (k < m) acc[2 + k] += c[k] * (double)tt;
+      for (int k = 0; k < kMaxSub; k++)
+        if (k < m) acc[2 + k] += c[k] * (double)tt;
+      acc[kMaxVec - 1] += (double)tt * (double)tt;
+    }
   }
-  block_reduce_store<kMaxVec>(acc, 2 + m, partials, gridDim.x);
+  block_reduce_store<kMaxVec>(acc, kMaxVec, partials, gridDim.x);
 }
 
 // t -= sum_k o_k C_k ; partials: [0] = t.t, [1+k] = C_k . t (for a second Gram-Schmidt round)
@@ -203,7 +207,9 @@ int residual_step(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, double 
   TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 1) * nb + kMaxVec));
   residual_kernel<T><<<nb, kVecThreads, 0, h->stream>>>(a, n, h->d_partials);
   TPB_LAUNCHED(h);
-  return finish_reduce(h, 2 + a.m, out);
+  TPB_CHECK(finish_reduce(h, kMaxVec, out));
+  out[2 + a.m] = out[kMaxVec - 1];  // t.t right after the m overlaps
+  return SBD_TPB_OK;
 }
 
 template <typename T>

@@ -7,7 +7,7 @@ namespace sbdtpb {
 
 constexpr int kVecThreads = 256;
 constexpr int kMaxSub = 16;            // largest Davidson subspace handled by the fused kernels
-constexpr int kMaxVec = kMaxSub + 2;   // values reduced per pass
+constexpr int kMaxVec = kMaxSub + 3;   // values reduced per pass
 
 template <typename T>
 struct VecPtrs {
@@ -20,14 +20,15 @@ struct CoefArray {
 
 template <typename T>
 struct ResidualArgs {
-  VecPtrs<T> C, HC;
-  double u[kMaxSub];  // lowest Ritz vector in the subspace basis
+  VecPtrs<T> C, HC;   // stored subspace vectors S_k and sigma(S_k); true C_k = f_k S_k
+  double u[kMaxSub];  // Ritz coefficients already multiplied by the scale factors f_k
   int m;              // subspace size
   double e_shifted;   // Ritz value of (H - shift)
   double e0;          // Ritz value of H
-  const double *hii;  // FP64 diagonal
+  const double *hii;  // FP64 diagonal (FP64 vectors)
+  const float *hii32; // H_ii - H_00 in FP32 (FP32 vectors); e0 is then E - H_00
   T *W;               // Ritz vector out (may be null)
-  T *t;               // preconditioned correction out
+  T *t;               // preconditioned correction out (may be null: W only)
 };
 
 int vec_blocks(sbd_tpb_handle *h);
