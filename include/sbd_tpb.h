@@ -70,6 +70,11 @@ typedef struct sbd_tpb_params {
   int preconditioner;/* SBD_TPB_PRECOND_* */
   int verbose;       /* print the reference's " Davidson iteration" lines to stdout */
   int device;        /* CUDA device ordinal used by sbd_tpb_diag */
+  int symmetry;      /* 1 (default): when the alpha and beta string lists are identical and the
+                        start is the HF determinant, every correction vector is projected onto
+                        the alpha<->beta exchange-symmetric sector the start vector lies in
+                        (C = C^T in the separated convention), so rounding cannot steer the
+                        iteration to a lower state of the other sector; 0: off */
 } sbd_tpb_params;
 
 /* Fills p with the reference defaults (tpb/sbdiag.h:22-50) and SBD_TPB_FP64 / diagonal. */
@@ -98,6 +103,8 @@ typedef struct sbd_tpb_result {
   double *one_rdm;    /* [2*L*L]  onebody[s][i + L*j] (tpb/correlation.h:378-664) */
   double *two_rdm;    /* [4*L^4]  twobody[s+2t][...] in the reference layout */
   double seconds_tables, seconds_davidson, seconds_rdm, seconds_total;
+  int learned_steps;  /* Davidson corrections taken from the learned preconditioner */
+  int fallback_steps; /* steps that fell back to the diagonal after a learned step failed */
 } sbd_tpb_result;
 
 /* ---- one-shot driver: replaces sbd::tpb::diag (tpb/sbdiag.h:139-151, one rank, --method 0) */
@@ -183,13 +190,61 @@ SBD_TPB_API void *sbd_tpb_stream(sbd_tpb_handle *h);
 /* Timing of the last sigma call on the handle's stream (CUDA events), milliseconds. */
 SBD_TPB_API double sbd_tpb_last_sigma_ms(sbd_tpb_handle *h);
 
-/* Per-kernel device times (ms) of the last sigma call, in launch order: [0] row kernel
- * (diagonal, beta part, alpha-beta part), [1] alpha column-slab kernel.  Returns how many were
- * written (<= max_n) or a negative status. */
+/* Per-stage device times (ms) of the last sigma call, in launch order: [0] alpha pass (diagonal,
+ * alpha singles/doubles, C^T), [1] beta pass, [2] alpha-beta term (sparse kernel or dense
+ * gather/contract/scatter).  Returns how many were written (<= max_n) or a negative status. */
 SBD_TPB_API int sbd_tpb_last_sigma_kernels(sbd_tpb_handle *h, double *ms, int max_n);
 
 /* Number of kernel launches the library has issued on this handle (for accounting). */
 SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);
+
+/* ---- learned Davidson preconditioner ------------------------------------------------------
+ * No counterpart in the reference, whose only correction is the diagonal one
+ * t = r / (E0 - H_ii) (tpb/davidson.h:858-868).  A small MLP predicts a per-determinant factor:
+ *   t_i = d_i * (1 + y_i),  d_i = r_i / (E0 - H_ii),
+ *   y = w3 . gelu(W2 gelu(W1 x + b1) + b2) + b3   (hidden width 256, tanh-form GELU, BF16
+ *   weights and activations on tensor cores, FP32 accumulation),
+ * with x = [asinh(H_ii - E0)/4, asinh(1e4 r_i/|r|)/10, the occupations of the 24 alpha and 24
+ * beta orbitals n-12 .. n+11 around the Fermi level (orbitals below 0 read as occupied), 14
+ * zeros].  It is trained by the library's own forward/backward kernels on pairs (d_k, exact
+ * correction Psi - W_k) recorded from plain FP64 Davidson runs; w3 = b3 = 0 at creation, so an
+ * untrained network is exactly the diagonal preconditioner.  The parameter vector is FP32 in
+ * the order W1[256][64], b1[256], W2[256][256], b2[256], w3[256], b3. */
+typedef struct sbd_tpb_precond sbd_tpb_precond;
+#define SBD_TPB_MLP_HIDDEN 256
+#define SBD_TPB_MLP_FEATURES 64
+#define SBD_TPB_MLP_PARAMS 82689
+
+SBD_TPB_API int sbd_tpb_precond_create(int device, uint64_t seed, sbd_tpb_precond **out);
+SBD_TPB_API int sbd_tpb_precond_destroy(sbd_tpb_precond *p);
+/* Runs the plain FP64 diagonal Davidson of params on the handle's problem, recording every
+ * correction step, and turns each step into training pairs (importance-sampled, about
+ * samples_per_step determinants each) appended to set `role` (0 = training, 1 = held out).
+ * energy (may be NULL) receives the converged energy. */
+SBD_TPB_API int sbd_tpb_precond_collect(sbd_tpb_precond *p, sbd_tpb_handle *h, const sbd_tpb_params *params,
+                                        size_t samples_per_step, int role, double *energy);
+SBD_TPB_API int sbd_tpb_precond_num_samples(sbd_tpb_precond *p, int role, size_t *n);
+/* Adam on the training set, minibatches of `batch` (multiple of 128); loss is the weighted mean
+ * of (a (1 + y) - b)^2 / 2 with a = d/|d| and b the scaled exact correction. */
+SBD_TPB_API int sbd_tpb_precond_train(sbd_tpb_precond *p, int epochs, int batch, double lr, double *last_loss);
+/* Weighted squared error of the learned correction and of the diagonal one (y = 0) on a set. */
+SBD_TPB_API int sbd_tpb_precond_evaluate(sbd_tpb_precond *p, int role, double *loss_learned,
+                                         double *loss_diagonal);
+SBD_TPB_API int sbd_tpb_precond_get_params(sbd_tpb_precond *p, float *params, size_t n);
+SBD_TPB_API int sbd_tpb_precond_set_params(sbd_tpb_precond *p, const float *params, size_t n);
+/* One forward/backward pass of the training kernels on n host samples (x: n x 64 features,
+ * a, b, w per sample): grad (SBD_TPB_MLP_PARAMS floats) of 0.5/n sum w (a (1 + y) - b)^2, its
+ * loss and the outputs y.  For gradient checks. */
+SBD_TPB_API int sbd_tpb_precond_gradients(sbd_tpb_precond *p, size_t n, const float *x, const float *a,
+                                          const float *b, const float *w, float *grad, double *loss,
+                                          float *y);
+/* The fused inference kernel on the handle's determinants: t = d (1 + y) from d (host, FP64,
+ * separated convention, [na*nb]), E0 and |r|.  For parity tests. */
+SBD_TPB_API int sbd_tpb_precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, const double *d, double e0,
+                                      double rnorm, double *t);
+/* Attaches p (or NULL) to the handle: Davidson with preconditioner SBD_TPB_PRECOND_LEARNED uses
+ * it.  The handle does not own p. */
+SBD_TPB_API int sbd_tpb_set_preconditioner(sbd_tpb_handle *h, sbd_tpb_precond *p);
 
 #ifdef __cplusplus
 }

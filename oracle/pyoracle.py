@@ -79,8 +79,9 @@ def lib():
         L.orc_reorder_sign.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                       _f32p, _f32p, _f32p, _f32p]
+        L.orc_mlp_backward.restype = C.c_double
         L.orc_mlp_backward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
-                                       _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
+                                       _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
         _LIB = L
     return _LIB
 
@@ -229,3 +230,29 @@ class System:
 
 def reorder_sign(a: int, b: int) -> int:
     return lib().orc_reorder_sign(int(a), int(b))
+
+
+def _f32(x):
+    return np.ascontiguousarray(x, np.float32)
+
+
+def mlp_forward(x, W1, b1, W2, b2, w3, b3):
+    """y of the preconditioner MLP (orc_mlp_forward), x [n, din]."""
+    x, W1, b1, W2, b2, w3, b3 = (_f32(v) for v in (x, W1, b1, W2, b2, w3, b3))
+    n, din = x.shape
+    dh = W1.shape[0]
+    h1 = np.zeros((n, dh), np.float32)
+    h2 = np.zeros((n, dh), np.float32)
+    y = np.zeros(n, np.float32)
+    lib().orc_mlp_forward(n, din, dh, x, W1, b1, W2, b2, w3, b3, h1, h2, y)
+    return y
+
+
+def mlp_backward(x, a, b, w, W1, b1, W2, b2, w3, b3):
+    """(loss, [gW1, gb1, gW2, gb2, gw3, gb3]) of the weighted preconditioner loss (orc_mlp_backward)."""
+    x, a, b, w, W1, b1, W2, b2, w3, b3 = (_f32(v) for v in (x, a, b, w, W1, b1, W2, b2, w3, b3))
+    n, din = x.shape
+    dh = W1.shape[0]
+    g = [np.zeros(W1.shape), np.zeros(dh), np.zeros(W2.shape), np.zeros(dh), np.zeros(dh), np.zeros(1)]
+    loss = lib().orc_mlp_backward(n, din, dh, x, a, b, w, W1, b1, W2, b2, w3, b3, *g)
+    return loss, g

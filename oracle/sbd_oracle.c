@@ -860,10 +860,10 @@ void orc_mlp_forward(int n, int din, int dh, const float *x, const float *W1, co
   }
 }
 
-void orc_mlp_backward(int n, int din, int dh, const float *x, const float *t, const float *W1,
-                      const float *b1, const float *W2, const float *b2, const float *W3,
-                      const float *b3, double *gW1, double *gb1, double *gW2, double *gb2,
-                      double *gW3, double *gb3) {
+double orc_mlp_backward(int n, int din, int dh, const float *x, const float *a, const float *b,
+                        const float *w, const float *W1, const float *b1, const float *W2,
+                        const float *b2, const float *W3, const float *b3, double *gW1, double *gb1,
+                        double *gW2, double *gb2, double *gW3, double *gb3) {
   float *h1 = malloc((size_t)n * dh * sizeof(float));
   float *h2 = malloc((size_t)n * dh * sizeof(float));
   float *y = malloc((size_t)n * sizeof(float));
@@ -875,8 +875,11 @@ void orc_mlp_backward(int n, int din, int dh, const float *x, const float *t, co
   memset(gW3, 0, (size_t)dh * sizeof(double));
   gb3[0] = 0.0;
   double *d2 = malloc((size_t)dh * sizeof(double)), *d1 = malloc((size_t)dh * sizeof(double));
+  double loss = 0.0;
   for (int r = 0; r < n; r++) {
-    double dy = ((double)y[r] - t[r]) / n;
+    const double e = (double)a[r] * (1.0 + (double)y[r]) - (double)b[r];
+    loss += 0.5 * w[r] * e * e / n;
+    double dy = (double)w[r] * a[r] * e / n;
     const float *a1 = h1 + (size_t)r * dh, *a2 = h2 + (size_t)r * dh;
     gb3[0] += dy;
     for (int i = 0; i < dh; i++) {
@@ -902,4 +905,5 @@ void orc_mlp_backward(int n, int din, int dh, const float *x, const float *t, co
   free(h1);
   free(h2);
   free(y);
+  return loss;
 }

@@ -119,11 +119,13 @@ int orc_reorder_sign(uint64_t a, uint64_t b);
 void orc_mlp_forward(int n, int din, int dh, const float *x, const float *W1, const float *b1,
                      const float *W2, const float *b2, const float *W3, const float *b3,
                      float *h1_out, float *h2_out, float *y);
-/* Gradients of 0.5*sum((y - t)^2)/n with respect to all weights (fp64 accumulation). */
-void orc_mlp_backward(int n, int din, int dh, const float *x, const float *t, const float *W1,
-                      const float *b1, const float *W2, const float *b2, const float *W3,
-                      const float *b3, double *gW1, double *gb1, double *gW2, double *gb2,
-                      double *gW3, double *gb3);
+/* Gradients, with respect to all weights (fp64 accumulation), of the learned preconditioner's
+ * loss 0.5/n * sum_r w_r (a_r (1 + y_r) - b_r)^2 (a = diagonal correction, b = exact correction,
+ * w = sampling weight); returns the loss. */
+double orc_mlp_backward(int n, int din, int dh, const float *x, const float *a, const float *b,
+                        const float *w, const float *W1, const float *b1, const float *W2,
+                        const float *b2, const float *W3, const float *b3, double *gW1, double *gb1,
+                        double *gW2, double *gb2, double *gW3, double *gb3);
 
 #ifdef __cplusplus
 }

@@ -84,6 +84,7 @@ void sbd_tpb_default_params(sbd_tpb_params *p) {
   p->preconditioner = SBD_TPB_PRECOND_DIAGONAL;
   p->verbose = 0;
   p->device = 0;
+  p->symmetry = 1;
 }
 
 const char *sbd_tpb_last_error(void) { return g_last_error.c_str(); }

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "mlp.cuh"
 #include "tpb_common.cuh"
 #include "vecops.cuh"
 
@@ -93,7 +94,8 @@ struct DevVec {
 
 template <typename T>
 int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, double shift,
-              double *dWout, double *resid_out, int *nsigma_out, int *converged_out) {
+              double *dWout, double *resid_out, int *nsigma_out, int *converged_out, DavRecord *rec,
+              sbd_tpb_precond *learned, double *energy_out, int *learned_steps, int *fallback_steps) {
   const size_t n = h->ndet();
   const int nb = prm->max_nb;
   const int max_it = prm->max_it;
@@ -139,7 +141,15 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
   double norm_R = 0.0, ww = 1.0;
   int nsigma = 0, m_last = 0;
   bool converged = false, stop = false, w_current = false;
+  // alpha <-> beta exchange symmetry (C = C^T): the HF start lies in the symmetric sector and
+  // H preserves it, so corrections are projected back onto it (rounding would otherwise let the
+  // iteration drift to a lower state of the antisymmetric sector)
+  const bool sym = prm->symmetry && !W0 && h->astr == h->bstr;
   ResidualArgs<T> ra;
+  double energy = 0.0, prev_norm = 0.0;
+  bool prev_learned = false;
+  int nlearned = 0, nfallback = 0;
+  std::vector<int> rec_cycle;  // basis indices of the current cycle (recording)
   const auto t_start = std::chrono::steady_clock::now();
 
   for (int it = 0; it < max_it && !stop; it++) {
@@ -183,6 +193,38 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       m_last = ib + 1;
       ww = out[0];
       norm_R = std::sqrt(out[1] / ww);
+      energy = ra.e0;
+      bool recording = false;
+      if (rec && !last && (int)rec->d.size() < rec->max_steps) {
+        // keep d_k, E_k, |r_k| and the step's basis for training pairs (dperp after Gram-Schmidt)
+        recording = true;
+        if (ib == 0) {
+          float *c0 = nullptr;
+          TPB_CUDA(cudaMalloc(&c0, sizeof(float) * n));
+          rec->owned.push_back(c0);
+          TPB_CHECK((convert_vec<T, float>(h, S[0].p, c0, n)));
+          rec->vec.push_back(c0);
+          rec->scale.push_back(f[0]);
+          rec_cycle.assign(1, (int)rec->vec.size() - 1);
+        }
+        float *dk = nullptr;
+        TPB_CUDA(cudaMalloc(&dk, sizeof(float) * n));
+        rec->d.push_back(dk);
+        TPB_CHECK((convert_vec<T, float>(h, tnext, dk, n)));
+        rec->e0.push_back(ra.e0);
+        rec->rnorm.push_back(std::sqrt(out[1]));
+        rec->basis.push_back(rec_cycle);
+      }
+      // learned correction: used unless the previous step was a learned one that did not lower
+      // the residual, in which case this step falls back to the diagonal correction
+      bool use_learned = false;
+      if (learned && !last) {
+        const bool failed = ib > 0 && prev_learned && !(norm_R < prev_norm);
+        use_learned = !failed;
+        if (failed) nfallback++;
+      }
+      prev_learned = use_learned;
+      prev_norm = norm_R;
       if (prm->verbose) {
         std::printf(" Davidson iteration %d.%d (tol=%.16g):", it, ib, norm_R);
         for (int p = 0; p < std::min(ib + 1, 4); p++) std::printf(" %.16g", E[p] + shift);
@@ -193,6 +235,20 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         converged = true;
         stop = true;
         break;
+      }
+      if (use_learned) TPB_CHECK(precond_apply<T>(h, learned, tnext, ra.e0, std::sqrt(out[1])));
+      if (sym && !last) {
+        // the S_k are exactly symmetric, so S_k.t is unchanged by the projection; only t.t is
+        TPB_CHECK(symmetrize<T>(h, tnext, &out[2 + ib + 1]));
+      }
+      if (use_learned) {
+        // overlaps S_k.t and t.t of the learned correction for the Gram-Schmidt below
+        std::vector<const T *> xp(ib + 2);
+        for (int k = 0; k <= ib; k++) xp[k] = S[k].p;
+        xp[ib + 1] = tnext;
+        TPB_CHECK(multi_dot<T>(h, xp.data(), ib + 2, tnext, n, dots.data()));
+        for (int k = 0; k <= ib + 1; k++) out[2 + k] = dots[k];
+        nlearned++;
       }
       if (!last) {
         // classical Gram-Schmidt against C_0..C_ib: t -= sum_k (C_k.t) C_k = sum_k f_k^2 (S_k.t) S_k.
@@ -215,6 +271,15 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
           break;
         }
         f[ib + 1] = 1.0 / std::sqrt(tt);
+        if (recording) {
+          float *dp = nullptr;
+          TPB_CUDA(cudaMalloc(&dp, sizeof(float) * n));
+          rec->dperp.push_back(dp);
+          TPB_CHECK((convert_vec<T, float>(h, tnext, dp, n)));
+          rec->vec.push_back(dp);
+          rec->scale.push_back(f[ib + 1]);
+          rec_cycle.push_back((int)rec->vec.size() - 1);
+        }
       }
       // max_time guard (tpb/davidson.h:887-913): stop when the next step would overrun
       TPB_CUDA(cudaStreamSynchronize(h->stream));
@@ -252,6 +317,9 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
   *resid_out = norm_R;
   *nsigma_out = nsigma;
   *converged_out = converged ? 1 : 0;
+  if (energy_out) *energy_out = energy;
+  if (learned_steps) *learned_steps = nlearned;
+  if (fallback_steps) *fallback_steps = nfallback;
   return SBD_TPB_OK;
 }
 
@@ -267,15 +335,27 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   const auto t0 = std::chrono::steady_clock::now();
   double resid = 0.0;
   int nsig = 0, conv = 0;
+  sbd_tpb_precond *learned = nullptr;
+  if (p->preconditioner == SBD_TPB_PRECOND_LEARNED) {
+    learned = h->precond;
+    if (!learned)
+      return fail(SBD_TPB_ERR_STATE, "davidson: learned preconditioner requested but none attached "
+                                     "(sbd_tpb_set_preconditioner)");
+  } else if (p->preconditioner != SBD_TPB_PRECOND_DIAGONAL) {
+    return fail(SBD_TPB_ERR_INVALID, "davidson: unknown preconditioner");
+  }
+  int nl = 0, nf = 0;
   DevVec<double> dW, dHW;
   TPB_CUDA(cudaMalloc(&dW.p, sizeof(double) * n));
   if (p->precision == SBD_TPB_MIXED) {
     double h00 = 0.0;
     TPB_CUDA(cudaMemcpy(&h00, h->d_hii, sizeof(double), cudaMemcpyDeviceToHost));
-    TPB_CHECK(run_typed<float>(h, p, W0, h00, dW.p, &resid, &nsig, &conv));
+    TPB_CHECK(run_typed<float>(h, p, W0, h00, dW.p, &resid, &nsig, &conv, nullptr, learned, nullptr, &nl, &nf));
   } else {
-    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, dW.p, &resid, &nsig, &conv));
+    TPB_CHECK(run_typed<double>(h, p, W0, 0.0, dW.p, &resid, &nsig, &conv, nullptr, learned, nullptr, &nl, &nf));
   }
+  res->learned_steps = nl;
+  res->fallback_steps = nf;
   // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
   TPB_CUDA(cudaMalloc(&dHW.p, sizeof(double) * n));
   double E = 0.0, rr = 0.0;
@@ -299,6 +379,21 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   res->converged = conv;
   res->seconds_davidson = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return conv ? SBD_TPB_OK : SBD_TPB_ERR_NOT_CONVERGED;
+}
+
+int davidson_record(sbd_tpb_handle *h, const sbd_tpb_params *p, DavRecord *rec, double *Psi,
+                    double *energy) {
+  if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "davidson: tables not built");
+  if (p->max_nb < 2 || p->max_nb > kMaxSub)
+    return fail(SBD_TPB_ERR_INVALID, "davidson: --block must be in [2, 16] for recording");
+  if (p->max_it < 1) return fail(SBD_TPB_ERR_INVALID, "davidson: --iteration must be >= 1");
+  double resid = 0.0;
+  int nsig = 0, conv = 0;
+  TPB_CHECK(run_typed<double>(h, p, nullptr, 0.0, Psi, &resid, &nsig, &conv, rec, nullptr, energy, nullptr,
+                              nullptr));
+  // a step that ended the run (converged, or nothing left to add) has no dperp
+  while (rec->dperp.size() < rec->d.size()) rec->dperp.push_back(nullptr);
+  return SBD_TPB_OK;
 }
 
 }  // namespace sbdtpb

@@ -249,6 +249,80 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
   }
 }
 
+// Alpha-single x beta-single terms when both singles tables are sparse:
+//   sigma[Ia, Ib] += sum_{(Ja, pq, sa) in S_a(Ia)} sum_{(Jb, rs, sb) in S_b(Ib)} sa sb (pq|rs) C[Ja, Jb]
+// One CTA per alpha row Ia that has singles.  For a group of its singles the CTA stages in shared
+// memory the whole ket rows C[Ja] and the integral rows sa (pq|.) (sign folded in), so the
+// scattered reads C[Ja, Jb] and (pq|rs) at the beta singles are shared-memory reads; each thread
+// owns a set of beta columns Ib that have singles and adds its sum into sigma[Ia, Ib] once per
+// group.  Groups are sized so several CTAs fit on an SM.  Without room for one row (kStage
+// false) the same loop reads C and the integrals through L1/L2.
+struct AbSparseArgs {
+  const uint32_t *rows;  // alpha rows with at least one single
+  const uint32_t *cols;  // beta columns with at least one single (ascending)
+  uint32_t ncols_s;
+  const uint32_t *as_off, *as_ket;
+  const int32_t *as_pair;  // +-(pq + 1), sign = alpha sign
+  const uint32_t *bs_off, *bs_ket;
+  const int32_t *bs_pair;  // +-(rs + 1), sign = beta sign
+  const double *eri;       // (pq|rs) [L*L][L*L]
+  int L2;
+  uint32_t nb;     // row length of C and sigma
+  uint32_t group;  // singles staged per round
+};
+
+template <typename T, bool kStage>
+__global__ void __launch_bounds__(256)
+    ab_sparse_kernel(AbSparseArgs a, const T *__restrict__ C, T *__restrict__ sigma) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *rows = reinterpret_cast<T *>(smem_raw);                // [group][nb]
+  T *gint = rows + (size_t)a.group * a.nb;                  // [group][L2], sign folded in
+  const uint32_t ia = __ldg(&a.rows[blockIdx.x]);
+  const uint32_t e0 = __ldg(&a.as_off[ia]), e1 = __ldg(&a.as_off[ia + 1]);
+  T *srow = sigma + (size_t)ia * a.nb;
+  for (uint32_t g0 = e0; g0 < e1; g0 += a.group) {
+    const uint32_t g1 = min(e1, g0 + a.group), ng = g1 - g0;
+    if (kStage) {
+      __syncthreads();
+      for (uint32_t j = 0; j < ng; j++) {
+        const T *src = C + (size_t)__ldg(&a.as_ket[g0 + j]) * a.nb;
+        T *dst = rows + (size_t)j * a.nb;
+        for (uint32_t c = threadIdx.x; c < a.nb; c += blockDim.x) dst[c] = __ldg(&src[c]);
+        const int32_t pa = __ldg(&a.as_pair[g0 + j]);
+        const double *erow = a.eri + (size_t)((pa > 0 ? pa : -pa) - 1) * a.L2;
+        T *gdst = gint + (size_t)j * a.L2;
+        for (int c = threadIdx.x; c < a.L2; c += blockDim.x) {
+          const double g = __ldg(&erow[c]);
+          gdst[c] = (T)(pa > 0 ? g : -g);
+        }
+      }
+      __syncthreads();
+    }
+    for (uint32_t q = threadIdx.x; q < a.ncols_s; q += blockDim.x) {
+      const uint32_t ib = __ldg(&a.cols[q]);
+      const uint32_t f0 = __ldg(&a.bs_off[ib]), f1 = __ldg(&a.bs_off[ib + 1]);
+      double acc = 0.0;
+      for (uint32_t f = f0; f < f1; f++) {
+        const uint32_t jb = __ldg(&a.bs_ket[f]);
+        const int32_t pb = __ldg(&a.bs_pair[f]);
+        const int rs = (pb > 0 ? pb : -pb) - 1;
+        double sum = 0.0;
+        for (uint32_t j = 0; j < ng; j++) {
+          if (kStage) {
+            sum += (double)gint[(size_t)j * a.L2 + rs] * (double)rows[(size_t)j * a.nb + jb];
+          } else {
+            const int32_t pa = __ldg(&a.as_pair[g0 + j]);
+            const double g = __ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
+            sum += (pa > 0 ? g : -g) * (double)__ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + jb]);
+          }
+        }
+        acc += pb > 0 ? sum : -sum;
+      }
+      srow[ib] = (T)((double)srow[ib] + acc);
+    }
+  }
+}
+
 __global__ void reorder_sign_kernel_f64(const uint64_t *__restrict__ apar,
                                         const uint64_t *__restrict__ bstr, uint32_t nb, size_t n,
                                         const double *__restrict__ x, double *__restrict__ y) {
@@ -318,6 +392,77 @@ uint32_t max_block_entries(const ExTable &t, size_t n) {
   return mx;
 }
 
+// Host-side facts about the tables that size the sigma launches: the most table entries of any
+// kBlkRows-row block (shared-memory staging) and, when want_ab_lists, the alpha rows and beta
+// columns that have singles (the sparse alpha-beta launch).  Computed once per table build.
+int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
+  const size_t na = h->astr.size(), nb = h->bstr.size();
+  if (h->blk_for != (const void *)h->ta_d.ket) {
+    h->blk_max[0] = max_block_entries(h->ta_d, na);
+    h->blk_max[1] = max_block_entries(h->ta_s, na);
+    h->blk_max[2] = max_block_entries(h->tb_d, nb);
+    h->blk_max[3] = max_block_entries(h->tb_s, nb);
+    h->blk_for = h->ta_d.ket;
+  }
+  if (want_ab_lists && !h->d_ab_rows && na > 0 && nb > 0) {
+    std::vector<uint32_t> ao(na + 1), bo(nb + 1), rows, cols;
+    TPB_CUDA(cudaMemcpy(ao.data(), h->ta_s.off, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToHost));
+    TPB_CUDA(cudaMemcpy(bo.data(), h->tb_s.off, sizeof(uint32_t) * (nb + 1), cudaMemcpyDeviceToHost));
+    uint32_t kmax = 0;
+    for (size_t i = 0; i < na; i++)
+      if (ao[i + 1] > ao[i]) {
+        rows.push_back((uint32_t)i);
+        kmax = std::max(kmax, ao[i + 1] - ao[i]);
+      }
+    for (size_t i = 0; i < nb; i++)
+      if (bo[i + 1] > bo[i]) cols.push_back((uint32_t)i);
+    TPB_CUDA(cudaMalloc(&h->d_ab_rows, sizeof(uint32_t) * std::max<size_t>(1, rows.size())));
+    TPB_CUDA(cudaMalloc(&h->d_ab_cols, sizeof(uint32_t) * std::max<size_t>(1, cols.size())));
+    if (!rows.empty())
+      TPB_CUDA(cudaMemcpy(h->d_ab_rows, rows.data(), sizeof(uint32_t) * rows.size(), cudaMemcpyHostToDevice));
+    if (!cols.empty())
+      TPB_CUDA(cudaMemcpy(h->d_ab_cols, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice));
+    h->ab_nrows = (uint32_t)rows.size();
+    h->ab_ncols = (uint32_t)cols.size();
+    h->ab_max_k = kmax;
+  }
+  return SBD_TPB_OK;
+}
+
+template <typename T>
+int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
+  if (h->ab_nrows == 0 || h->ab_ncols == 0) return SBD_TPB_OK;
+  AbSparseArgs a{};
+  a.rows = h->d_ab_rows;
+  a.cols = h->d_ab_cols;
+  a.ncols_s = h->ab_ncols;
+  a.as_off = h->ta_s.off;
+  a.as_ket = h->ta_s.ket;
+  a.as_pair = h->pa.s_pair;
+  a.bs_off = h->tb_s.off;
+  a.bs_ket = h->tb_s.ket;
+  a.bs_pair = h->pb.s_pair;
+  a.eri = h->d_eri;
+  a.L2 = h->L * h->L;
+  a.nb = (uint32_t)h->bstr.size();
+  // one staged single = its C row and its integral row; aim for 4 CTAs per SM, else as many
+  // singles as fit in one CTA's shared memory
+  const size_t per = ((size_t)a.nb + a.L2) * sizeof(T);
+  const size_t target = std::max<size_t>(per, h->smem_optin / 4 - 1024);
+  if (per <= h->smem_optin) {
+    a.group = (uint32_t)std::max<size_t>(1, std::min<size_t>(target / per, h->ab_max_k));
+    const size_t smem = a.group * per;
+    TPB_CUDA(cudaFuncSetAttribute(ab_sparse_kernel<T, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ab_sparse_kernel<T, true><<<h->ab_nrows, 256, smem, h->stream>>>(a, C, sigma);
+  } else {
+    a.group = h->ab_max_k;
+    ab_sparse_kernel<T, false><<<h->ab_nrows, 256, 0, h->stream>>>(a, C, sigma);
+  }
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
 template <typename T>
 int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, double shift) {
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
@@ -331,13 +476,7 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
     h->ct_bytes = n * sizeof(double);
   }
   T *CT = reinterpret_cast<T *>(h->d_ct);
-  if (h->blk_for != (const void *)h->ta_d.ket) {
-    h->blk_max[0] = max_block_entries(h->ta_d, na);
-    h->blk_max[1] = max_block_entries(h->ta_s, na);
-    h->blk_max[2] = max_block_entries(h->tb_d, nb);
-    h->blk_max[3] = max_block_entries(h->tb_s, nb);
-    h->blk_for = h->ta_d.ket;
-  }
+  TPB_CHECK(prepare_sigma_meta(h, !dense_ab));
 
   BlockArgs ba{};
   ba.s_off = h->ta_s.off;
@@ -360,7 +499,7 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   ba.hii32 = h->d_hii32;
   ba.core_shift = sizeof(T) == 8 ? shift : h->h00 - shift;
   ba.accumulate = accumulate;
-  ba.do_ab = dense_ab ? 0 : 1;
+  ba.do_ab = 0;  // alpha-beta terms: dense path or the sparse kernel below
   ba.bs_off = h->tb_s.off;
   ba.bs_ket = h->tb_s.ket;
   ba.bs_pair = h->pb.s_pair;
@@ -388,8 +527,13 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   bb.max_s = h->blk_max[3];
   TPB_CHECK((launch_block<T, false>(h, bb, CT, sigma, nullptr)));
   TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
-  h->sigma_kernels = 2;
-  if (dense_ab) TPB_CHECK(ab_dense_apply<T>(h, C, sigma));
+  if (dense_ab) {
+    TPB_CHECK(ab_dense_apply<T>(h, C, sigma));
+  } else {
+    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma));
+  }
+  TPB_CUDA(cudaEventRecord(h->ev_k[2], h->stream));
+  h->sigma_kernels = 3;
   TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
   return SBD_TPB_OK;
 }
@@ -399,13 +543,7 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
 template <typename T>
 int sigma_sep_given_ct(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, T *CT) {
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
-  if (h->blk_for != (const void *)h->ta_d.ket) {
-    h->blk_max[0] = max_block_entries(h->ta_d, na);
-    h->blk_max[1] = max_block_entries(h->ta_s, na);
-    h->blk_max[2] = max_block_entries(h->tb_d, nb);
-    h->blk_max[3] = max_block_entries(h->tb_s, nb);
-    h->blk_for = h->ta_d.ket;
-  }
+  TPB_CHECK(prepare_sigma_meta(h, false));
   BlockArgs ba{};
   ba.s_off = h->ta_s.off;
   ba.s_ket = h->ta_s.ket;

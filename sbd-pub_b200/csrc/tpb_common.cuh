@@ -161,6 +161,13 @@ struct sbd_tpb_handle {
   size_t ct_bytes = 0;
   void *d_ab_work = nullptr;     // dense alpha-beta intermediates
   size_t ab_work_bytes = 0;
+  // sparse alpha-beta term: alpha rows and beta columns that have at least one single
+  uint32_t *d_ab_rows = nullptr, *d_ab_cols = nullptr;
+  uint32_t ab_nrows = 0, ab_ncols = 0, ab_max_k = 0;  // ab_max_k: most singles of one alpha row
+  // learned preconditioner attached by sbd_tpb_set_preconditioner (not owned) and the
+  // occupation windows of the strings it reads
+  struct sbd_tpb_precond *precond = nullptr;
+  uint32_t *d_occw_a = nullptr, *d_occw_b = nullptr;
   size_t ndet() const { return astr.size() * bstr.size(); }
 };
 

@@ -8,6 +8,7 @@
 // storage type, per block in a fixed order, and the block partials are summed in a fixed order
 // by a second kernel, so every reduction is run-to-run deterministic.
 #include <algorithm>
+#include <type_traits>
 
 #include "tpb_common.cuh"
 #include "vecops.cuh"
@@ -35,20 +36,72 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], int nv, doub
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads)
-    multi_dot_kernel(VecPtrs<T> X, int k, const T *__restrict__ y, size_t n, double *partials) {
-  double acc[kMaxVec];
+// W consecutive elements: one 16-byte access when W = 16 / sizeof(T), scalars when W = 1 (tail)
+template <typename T, int W>
+__device__ __forceinline__ void ldv(const T *__restrict__ p, T (&v)[W]) {
+  if constexpr (W == 4 && sizeof(T) == 4) {
+    const float4 f = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
+  } else if constexpr (W == 2 && sizeof(T) == 8) {
+    const double2 f = __ldg(reinterpret_cast<const double2 *>(p));
+    v[0] = f.x, v[1] = f.y;
+  } else {
 #pragma unroll
-  for (int j = 0; j < kMaxVec; j++) acc[j] = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double yi = (double)y[i];
-#pragma unroll
-    for (int j = 0; j < kMaxVec; j++)
-      if (j < k) acc[j] += (double)X.p[j][i] * yi;
+    for (int l = 0; l < W; l++) v[l] = __ldg(p + l);
   }
-  block_reduce_store<kMaxVec>(acc, k, partials, gridDim.x);
+}
+template <typename T, int W>
+__device__ __forceinline__ void stv(T *__restrict__ p, const T (&v)[W]) {
+  if constexpr (W == 4 && sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (W == 2 && sizeof(T) == 8) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  } else {
+#pragma unroll
+    for (int l = 0; l < W; l++) p[l] = v[l];
+  }
+}
+
+// Every vector pass walks the vectors in 16-byte groups (grid-stride), and block 0 finishes the
+// n % VW tail element by element; `body<W>(i)` handles elements i .. i+W-1.
+template <typename T, typename Body>
+__device__ __forceinline__ void for_each_group(size_t n, Body &&body) {
+  constexpr int VW = 16 / sizeof(T);
+  const size_t ng = n / VW;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < ng; g += (size_t)gridDim.x * blockDim.x)
+    body.template run<VW>(g * VW);
+  if (blockIdx.x == 0 && threadIdx.x < n - ng * VW) body.template run<1>(ng * VW + threadIdx.x);
+}
+
+// out[j] = X_j . y, j < K
+template <typename T, int K>
+struct DotBody {
+  const VecPtrs<T> &X;
+  const T *y;
+  double (&acc)[K];
+  template <int W>
+  __device__ __forceinline__ void run(size_t i) {
+    T yv[W];
+    ldv<T, W>(y + i, yv);
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      T xv[W];
+      ldv<T, W>(X.p[j] + i, xv);
+#pragma unroll
+      for (int l = 0; l < W; l++) acc[j] += (double)xv[l] * (double)yv[l];
+    }
+  }
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kVecThreads)
+    multi_dot_kernel(VecPtrs<T> X, const T *__restrict__ y, size_t n, double *partials) {
+  double acc[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) acc[j] = 0.0;
+  DotBody<T, K> b{X, y, acc};
+  for_each_group<T>(n, b);
+  block_reduce_store<K>(acc, K, partials, gridDim.x);
 }
 
 __global__ void reduce_partials_kernel(const double *__restrict__ partials, int nblocks,
@@ -67,74 +120,107 @@ __global__ void reduce_partials_kernel(const double *__restrict__ partials, int 
 }
 
 // W = sum_k u_k S_k ; r = E' W - sum_k u_k sigma(S_k) ; t = r / (E0 - H_ii) (regularised as
-// tpb/davidson.h:861-868) ; partials: [0] = W.W, [1] = r.r, [2+k] = S_k . t, [2+m] = t.t
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads)
-    residual_kernel(ResidualArgs<T> a, size_t n, double *partials) {
-  double acc[kMaxVec];
+// tpb/davidson.h:861-868) ; partials: [0] = W.W, [1] = r.r, [2+k] = S_k . t, [2+M] = t.t
+template <typename T, int M>
+struct ResidualBody {
+  const ResidualArgs<T> &a;
+  double (&acc)[M + 3];
+  template <int W>
+  __device__ __forceinline__ void run(size_t i) {
+    T c[M][W];
+    double w[W], hc[W];
 #pragma unroll
-  for (int j = 0; j < kMaxVec; j++) acc[j] = 0.0;
-  const int m = a.m;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    double c[kMaxSub];
-    double w = 0.0, hc = 0.0;
+    for (int l = 0; l < W; l++) w[l] = hc[l] = 0.0;
 #pragma unroll
-    for (int k = 0; k < kMaxSub; k++) {
-      if (k < m) {
-        c[k] = (double)a.C.p[k][i];
-        w += a.u[k] * c[k];
-        hc += a.u[k] * (double)a.HC.p[k][i];
+    for (int k = 0; k < M; k++) {
+      T hv[W];
+      ldv<T, W>(a.C.p[k] + i, c[k]);
+      ldv<T, W>(a.HC.p[k] + i, hv);
+#pragma unroll
+      for (int l = 0; l < W; l++) {
+        w[l] += a.u[k] * (double)c[k][l];
+        hc[l] += a.u[k] * (double)hv[l];
       }
     }
-    const double r = a.e_shifted * w - hc;
-    if (a.W) a.W[i] = (T)w;
-    acc[0] += w * w;
-    acc[1] += r * r;
-    if (a.t) {
-      const double hd = a.hii32 ? (double)a.hii32[i] : a.hii[i];
-      const double d = a.e0 - hd;
-      const double t = (fabs(d) > 1.0e-12) ? r / d : r / (d - 1.0e-12);
-      const T tt = (T)t;
-      a.t[i] = tt;
+    T wt[W], tt[W];
 #pragma unroll
-      for (int k = 0; k < kMaxSub; k++)
-        if (k < m) acc[2 + k] += c[k] * (double)tt;
-      acc[kMaxVec - 1] += (double)tt * (double)tt;
+    for (int l = 0; l < W; l++) {
+      const double r = a.e_shifted * w[l] - hc[l];
+      wt[l] = (T)w[l];
+      acc[0] += w[l] * w[l];
+      acc[1] += r * r;
+      if (a.t) {
+        const double hd = a.hii32 ? (double)__ldg(&a.hii32[i + l]) : __ldg(&a.hii[i + l]);
+        const double d = a.e0 - hd;
+        tt[l] = (T)((fabs(d) > 1.0e-12) ? r / d : r / (d - 1.0e-12));
+      }
+    }
+    if (a.W) stv<T, W>(a.W + i, wt);
+    if (a.t) {
+      stv<T, W>(a.t + i, tt);
+#pragma unroll
+      for (int l = 0; l < W; l++) {
+#pragma unroll
+        for (int k = 0; k < M; k++) acc[2 + k] += (double)c[k][l] * (double)tt[l];
+        acc[2 + M] += (double)tt[l] * (double)tt[l];
+      }
     }
   }
-  block_reduce_store<kMaxVec>(acc, kMaxVec, partials, gridDim.x);
+};
+
+template <typename T, int M>
+__global__ void __launch_bounds__(kVecThreads) residual_kernel(ResidualArgs<T> a, size_t n, double *partials) {
+  double acc[M + 3];
+#pragma unroll
+  for (int j = 0; j < M + 3; j++) acc[j] = 0.0;
+  ResidualBody<T, M> b{a, acc};
+  for_each_group<T>(n, b);
+  block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
 }
 
 // t -= sum_k o_k C_k ; partials: [0] = t.t, [1+k] = C_k . t (for a second Gram-Schmidt round)
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads)
-    cgs_update_kernel(VecPtrs<T> C, int m, CoefArray o, T *__restrict__ t, size_t n,
-                      double *partials, int want_dots) {
-  double acc[kMaxVec];
+template <typename T, int M, bool kDots>
+struct CgsBody {
+  const VecPtrs<T> &C;
+  const CoefArray &o;
+  T *t;
+  double (&acc)[M + 1];
+  template <int W>
+  __device__ __forceinline__ void run(size_t i) {
+    T tv[W], c[M][W];
+    ldv<T, W>(t + i, tv);
+    double x[W];
 #pragma unroll
-  for (int j = 0; j < kMaxVec; j++) acc[j] = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    double c[kMaxSub];
-    double x = (double)t[i];
+    for (int l = 0; l < W; l++) x[l] = (double)tv[l];
 #pragma unroll
-    for (int k = 0; k < kMaxSub; k++) {
-      if (k < m) {
-        c[k] = (double)C.p[k][i];
-        x -= o.v[k] * c[k];
+    for (int k = 0; k < M; k++) {
+      ldv<T, W>(C.p[k] + i, c[k]);
+#pragma unroll
+      for (int l = 0; l < W; l++) x[l] -= o.v[k] * (double)c[k][l];
+    }
+    T xt[W];
+#pragma unroll
+    for (int l = 0; l < W; l++) {
+      xt[l] = (T)x[l];
+      acc[0] += (double)xt[l] * (double)xt[l];
+      if (kDots) {
+#pragma unroll
+        for (int k = 0; k < M; k++) acc[1 + k] += (double)c[k][l] * (double)xt[l];
       }
     }
-    const T xt = (T)x;
-    t[i] = xt;
-    acc[0] += (double)xt * (double)xt;
-    if (want_dots) {
-#pragma unroll
-      for (int k = 0; k < kMaxSub; k++)
-        if (k < m) acc[1 + k] += c[k] * (double)xt;
-    }
+    stv<T, W>(t + i, xt);
   }
-  block_reduce_store<kMaxVec>(acc, want_dots ? 1 + m : 1, partials, gridDim.x);
+};
+
+template <typename T, int M, bool kDots>
+__global__ void __launch_bounds__(kVecThreads)
+    cgs_update_kernel(VecPtrs<T> C, CoefArray o, T *__restrict__ t, size_t n, double *partials) {
+  double acc[M + 1];
+#pragma unroll
+  for (int j = 0; j < M + 1; j++) acc[j] = 0.0;
+  CgsBody<T, M, kDots> b{C, o, t, acc};
+  for_each_group<T>(n, b);
+  block_reduce_store<M + 1>(acc, kDots ? M + 1 : 1, partials, gridDim.x);
 }
 
 template <typename T>
@@ -160,6 +246,50 @@ __global__ void axpby_kernel(const T *__restrict__ x, T *__restrict__ y, double 
     y[i] = (T)(a * (double)x[i] + b * (double)y[i]);
 }
 
+// t <- (t + t^T) / 2 for a square nb x nb vector (alpha and beta strings identical), in place,
+// one 32 x 32 tile pair (bi <= bj) at a time; partials[block] = sum of the new t^2 over the
+// block's tile pairs (fixed assignment, so the sum is deterministic).
+template <typename T>
+__global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint32_t nb, double *partials) {
+  __shared__ T A[32][33], B[32][33];
+  const uint32_t T_ = (nb + 31) / 32;
+  const size_t npairs = (size_t)T_ * T_;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  double acc = 0.0;
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const uint32_t bi = (uint32_t)(p / T_), bj = (uint32_t)(p % T_);
+    if (bi > bj) continue;
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const uint32_t i = bi * 32 + r, j = bj * 32 + tx;
+      A[r][tx] = (i < nb && j < nb) ? t[(size_t)i * nb + j] : T(0);
+      const uint32_t i2 = bj * 32 + r, j2 = bi * 32 + tx;
+      B[r][tx] = (i2 < nb && j2 < nb) ? t[(size_t)i2 * nb + j2] : T(0);
+    }
+    __syncthreads();
+    const double mult = bi == bj ? 1.0 : 2.0;
+    for (int r = ty; r < 32; r += 8) {
+      // new A[r][c] = (A[r][c] + B[c][r]) / 2, written to both (i, j) and (j, i)
+      const uint32_t i = bi * 32 + r, j = bj * 32 + tx;
+      const T v = (T)(((double)A[r][tx] + (double)B[tx][r]) * 0.5);
+      if (i < nb && j < nb) {
+        t[(size_t)i * nb + j] = v;
+        acc += mult * (double)v * (double)v;
+      }
+    }
+    __syncthreads();
+    if (bi != bj) {
+      for (int r = ty; r < 32; r += 8) {
+        const uint32_t i2 = bj * 32 + r, j2 = bi * 32 + tx;
+        const T v = (T)(((double)A[tx][r] + (double)B[r][tx]) * 0.5);
+        if (i2 < nb && j2 < nb) t[(size_t)i2 * nb + j2] = v;
+      }
+    }
+  }
+  double v[1] = {acc};
+  block_reduce_store<1>(v, 1, partials, gridDim.x);
+}
+
 }  // namespace
 
 int ensure_partials(sbd_tpb_handle *h, size_t n) {
@@ -176,7 +306,7 @@ int vec_blocks(sbd_tpb_handle *h) { return h->num_sms * 4; }
 
 static int finish_reduce(sbd_tpb_handle *h, int nvals, double *host_out) {
   const int nb = vec_blocks(h);
-  double *d_out = h->d_partials + (size_t)kMaxVec * nb;
+  double *d_out = h->d_partials + (size_t)(kMaxVec + 3) * nb;
   reduce_partials_kernel<<<nvals, 256, 0, h->stream>>>(h->d_partials, nb, d_out);
   TPB_LAUNCHED(h);
   TPB_CUDA(cudaMemcpyAsync(host_out, d_out, sizeof(double) * nvals, cudaMemcpyDeviceToHost,
@@ -185,16 +315,30 @@ static int finish_reduce(sbd_tpb_handle *h, int nvals, double *host_out) {
   return SBD_TPB_OK;
 }
 
+// compile-time subspace size from a runtime one (1 .. kMaxVec)
+template <int N, typename F>
+int dispatch_n(int n, F &&f) {
+  if constexpr (N > kMaxVec) {
+    return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  } else {
+    if (n == N) return f(std::integral_constant<int, N>());
+    return dispatch_n<N + 1>(n, f);
+  }
+}
+
 template <typename T>
 int multi_dot(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n, double *out) {
   const int nb = vec_blocks(h);
-  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 1) * nb + kMaxVec));
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
   for (int j0 = 0; j0 < k; j0 += kMaxVec) {
     const int kk = std::min(kMaxVec, k - j0);
     VecPtrs<T> P;
     for (int j = 0; j < kMaxVec; j++) P.p[j] = (j < kk) ? X[j0 + j] : nullptr;
-    multi_dot_kernel<T><<<nb, kVecThreads, 0, h->stream>>>(P, kk, y, n, h->d_partials);
-    TPB_LAUNCHED(h);
+    TPB_CHECK(dispatch_n<1>(kk, [&](auto K) {
+      multi_dot_kernel<T, decltype(K)::value><<<nb, kVecThreads, 0, h->stream>>>(P, y, n, h->d_partials);
+      TPB_LAUNCHED(h);
+      return SBD_TPB_OK;
+    }));
     TPB_CHECK(finish_reduce(h, kk, out + j0));
   }
   return SBD_TPB_OK;
@@ -202,29 +346,52 @@ int multi_dot(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n,
 
 template <typename T>
 int residual_step(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, double *out) {
-  if (a.m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  if (a.m < 1 || a.m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
   const int nb = vec_blocks(h);
-  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 1) * nb + kMaxVec));
-  residual_kernel<T><<<nb, kVecThreads, 0, h->stream>>>(a, n, h->d_partials);
-  TPB_LAUNCHED(h);
-  TPB_CHECK(finish_reduce(h, kMaxVec, out));
-  out[2 + a.m] = out[kMaxVec - 1];  // t.t right after the m overlaps
-  return SBD_TPB_OK;
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
+  TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      residual_kernel<T, M><<<nb, kVecThreads, 0, h->stream>>>(a, n, h->d_partials);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return finish_reduce(h, a.m + 3, out);  // [0] ww, [1] rr, [2..2+m) S_k.t, [2+m] t.t
 }
 
 template <typename T>
 int cgs_update(sbd_tpb_handle *h, const T *const *C, int m, const double *o, T *t, size_t n,
                int want_dots, double *out) {
-  if (m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
   const int nb = vec_blocks(h);
-  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 1) * nb + kMaxVec));
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
   VecPtrs<T> P;
   CoefArray co;
   for (int j = 0; j < kMaxVec; j++) P.p[j] = j < m ? C[j] : nullptr;
   for (int j = 0; j < kMaxSub; j++) co.v[j] = j < m ? o[j] : 0.0;
-  cgs_update_kernel<T><<<nb, kVecThreads, 0, h->stream>>>(P, m, co, t, n, h->d_partials, want_dots);
-  TPB_LAUNCHED(h);
+  TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      if (want_dots)
+        cgs_update_kernel<T, M, true><<<nb, kVecThreads, 0, h->stream>>>(P, co, t, n, h->d_partials);
+      else
+        cgs_update_kernel<T, M, false><<<nb, kVecThreads, 0, h->stream>>>(P, co, t, n, h->d_partials);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
   return finish_reduce(h, want_dots ? 1 + m : 1, out);
+}
+
+template <typename T>
+int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = vec_blocks(h);
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nblk + kMaxVec + 3));
+  symmetrize_kernel<T><<<nblk, 256, 0, h->stream>>>(t, nb, h->d_partials);
+  TPB_LAUNCHED(h);
+  return finish_reduce(h, 1, tt);
 }
 
 template <typename T>
@@ -259,10 +426,13 @@ template int cgs_update<double>(sbd_tpb_handle *, const double *const *, int, co
                                 double *, size_t, int, double *);
 template int cgs_update<float>(sbd_tpb_handle *, const float *const *, int, const double *,
                                float *, size_t, int, double *);
+template int symmetrize<double>(sbd_tpb_handle *, double *, double *);
+template int symmetrize<float>(sbd_tpb_handle *, float *, double *);
 template int scale_vec<double>(sbd_tpb_handle *, double *, double, size_t);
 template int scale_vec<float>(sbd_tpb_handle *, float *, double, size_t);
 template int convert_vec<double, float>(sbd_tpb_handle *, const double *, float *, size_t);
 template int convert_vec<float, double>(sbd_tpb_handle *, const float *, double *, size_t);
+template int convert_vec<float, float>(sbd_tpb_handle *, const float *, float *, size_t);
 template int axpby<double>(sbd_tpb_handle *, const double *, double *, double, double, size_t);
 template int axpby<float>(sbd_tpb_handle *, const float *, float *, double, double, size_t);
 

@@ -39,6 +39,9 @@ int cgs_update(sbd_tpb_handle *h, const T *const *C, int m, const double *o, T *
                int want_dots, double *out);
 template <typename T>
 int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n);
+// t <- (t + t^T)/2 over the square (alpha = beta strings) determinant matrix; tt = new t.t
+template <typename T>
+int symmetrize(sbd_tpb_handle *h, T *t, double *tt);
 template <typename S, typename D>
 int convert_vec(sbd_tpb_handle *h, const S *x, D *y, size_t n);
 template <typename T>

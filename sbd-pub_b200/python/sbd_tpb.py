@@ -39,7 +39,12 @@ EXPORTED = [
     "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
     "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_sigma_noalloc", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
     "sbd_tpb_last_sigma_ms", "sbd_tpb_last_sigma_kernels", "sbd_tpb_kernel_launches",
+    "sbd_tpb_precond_create", "sbd_tpb_precond_destroy", "sbd_tpb_precond_collect",
+    "sbd_tpb_precond_num_samples", "sbd_tpb_precond_train", "sbd_tpb_precond_evaluate",
+    "sbd_tpb_precond_get_params", "sbd_tpb_precond_set_params", "sbd_tpb_precond_gradients",
+    "sbd_tpb_precond_apply", "sbd_tpb_set_preconditioner",
 ]
+MLP_HIDDEN, MLP_FEATURES, MLP_PARAMS = 256, 64, 82689
 
 
 class TpbError(RuntimeError):
@@ -52,7 +57,7 @@ class Params(C.Structure):
     _fields_ = [
         ("max_it", C.c_int), ("max_nb", C.c_int), ("eps", C.c_double), ("max_time", C.c_double),
         ("init", C.c_int), ("do_rdm", C.c_int), ("precision", C.c_int), ("preconditioner", C.c_int),
-        ("verbose", C.c_int), ("device", C.c_int),
+        ("verbose", C.c_int), ("device", C.c_int), ("symmetry", C.c_int),
     ]
 
 
@@ -71,7 +76,7 @@ class Result(C.Structure):
         ("density", C.POINTER(C.c_double)), ("one_rdm", C.POINTER(C.c_double)),
         ("two_rdm", C.POINTER(C.c_double)), ("seconds_tables", C.c_double),
         ("seconds_davidson", C.c_double), ("seconds_rdm", C.c_double),
-        ("seconds_total", C.c_double),
+        ("seconds_total", C.c_double), ("learned_steps", C.c_int), ("fallback_steps", C.c_int),
     ]
 
 
@@ -112,6 +117,19 @@ def lib():
     L.sbd_tpb_last_sigma_kernels.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
     L.sbd_tpb_kernel_launches.restype = C.c_uint64
     L.sbd_tpb_kernel_launches.argtypes = [vp]
+    L.sbd_tpb_precond_create.argtypes = [C.c_int, C.c_uint64, C.POINTER(vp)]
+    L.sbd_tpb_precond_destroy.argtypes = [vp]
+    L.sbd_tpb_precond_collect.argtypes = [vp, vp, C.POINTER(Params), C.c_size_t, C.c_int,
+                                          C.POINTER(C.c_double)]
+    L.sbd_tpb_precond_num_samples.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t)]
+    L.sbd_tpb_precond_train.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double)]
+    L.sbd_tpb_precond_evaluate.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.sbd_tpb_precond_get_params.argtypes = [vp, vp, C.c_size_t]
+    L.sbd_tpb_precond_set_params.argtypes = [vp, vp, C.c_size_t]
+    L.sbd_tpb_precond_gradients.argtypes = [vp, C.c_size_t, vp, vp, vp, vp, vp,
+                                            C.POINTER(C.c_double), vp]
+    L.sbd_tpb_precond_apply.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp]
+    L.sbd_tpb_set_preconditioner.argtypes = [vp, vp]
     _lib = L
     return L
 
@@ -166,6 +184,7 @@ class Handle:
 
     def __init__(self, device: int = 0):
         self.h = C.c_void_p()
+        self.device = device
         _check(lib().sbd_tpb_create(device, C.byref(self.h)))
         self.problem: Problem | None = None
 
@@ -241,7 +260,7 @@ class Handle:
         return lib().sbd_tpb_last_sigma_ms(self.h)
 
     def last_sigma_kernels(self):
-        """Device ms of each kernel of the last sigma: [row kernel, alpha slab kernel]."""
+        """Device ms of each stage of the last sigma: [alpha pass, beta pass, alpha-beta term]."""
         buf = (C.c_double * 8)()
         n = lib().sbd_tpb_last_sigma_kernels(self.h, buf, 8)
         _check(n if n < 0 else OK)
@@ -273,7 +292,13 @@ class Handle:
         _check(rc, allow=(OK, ERR_NOT_CONVERGED))
         return dict(energy=res.energy, residual=res.residual, iterations=res.iterations,
                     converged=bool(res.converged), W=W, density=dens, one=one, two=two,
-                    seconds=res.seconds_davidson)
+                    seconds=res.seconds_davidson, learned_steps=res.learned_steps,
+                    fallback_steps=res.fallback_steps)
+
+    def set_preconditioner(self, pc: "Precond | None"):
+        """Attach a learned preconditioner (used when params.preconditioner == PRECOND_LEARNED)."""
+        _check(lib().sbd_tpb_set_preconditioner(self.h, pc.p if pc is not None else None))
+        self._pc = pc  # keep it alive while attached
 
     def rdm(self, W: np.ndarray, two_body=True):
         L = self.problem.norb
@@ -283,6 +308,92 @@ class Handle:
         _check(lib().sbd_tpb_rdm(self.h, w.ctypes.data, one.ctypes.data,
                                  two.ctypes.data if two is not None else None, HOST))
         return one, two
+
+
+class Precond:
+    """Learned Davidson preconditioner (MLP, trained by the library's own kernels)."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.p = C.c_void_p()
+        _check(lib().sbd_tpb_precond_create(device, seed, C.byref(self.p)))
+
+    def close(self):
+        if self.p:
+            lib().sbd_tpb_precond_destroy(self.p)
+            self.p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def collect(self, handle: Handle, params: Params | None = None, samples_per_step=1 << 17,
+                role=0) -> float:
+        """Plain FP64 Davidson on the handle's problem; its steps become training pairs."""
+        params = params or default_params(max_it=4, max_nb=10, eps=1e-8)
+        e = C.c_double()
+        _check(lib().sbd_tpb_precond_collect(self.p, handle.h, C.byref(params), samples_per_step,
+                                             role, C.byref(e)))
+        return e.value
+
+    def num_samples(self, role=0) -> int:
+        n = C.c_size_t()
+        _check(lib().sbd_tpb_precond_num_samples(self.p, role, C.byref(n)))
+        return n.value
+
+    def train(self, epochs=3, batch=8192, lr=1e-3) -> float:
+        loss = C.c_double()
+        _check(lib().sbd_tpb_precond_train(self.p, epochs, batch, lr, C.byref(loss)))
+        return loss.value
+
+    def evaluate(self, role=1):
+        """(learned, diagonal) weighted squared errors against the exact corrections of a set."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().sbd_tpb_precond_evaluate(self.p, role, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, np.float32)
+        _check(lib().sbd_tpb_precond_get_params(self.p, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, params: np.ndarray):
+        x = np.ascontiguousarray(params, np.float32)
+        _check(lib().sbd_tpb_precond_set_params(self.p, x.ctypes.data, x.size))
+
+    def gradients(self, x, a, b, w):
+        """One forward/backward pass of the training kernels: (grad, loss, y)."""
+        x = np.ascontiguousarray(x, np.float32)
+        a, b, w = (np.ascontiguousarray(v, np.float32) for v in (a, b, w))
+        n = len(a)
+        grad = np.zeros(MLP_PARAMS, np.float32)
+        y = np.zeros(n, np.float32)
+        loss = C.c_double()
+        _check(lib().sbd_tpb_precond_gradients(self.p, n, x.ctypes.data, a.ctypes.data, b.ctypes.data,
+                                               w.ctypes.data, grad.ctypes.data, C.byref(loss),
+                                               y.ctypes.data))
+        return grad, loss.value, y
+
+    def apply(self, handle: Handle, d: np.ndarray, e0: float, rnorm: float) -> np.ndarray:
+        """The fused inference kernel on the handle's determinants: t = d (1 + y)."""
+        d = np.ascontiguousarray(d, np.float64)
+        t = np.zeros_like(d)
+        _check(lib().sbd_tpb_precond_apply(handle.h, self.p, d.ctypes.data, e0, rnorm, t.ctypes.data))
+        return t
+
+
+def mlp_unpack(params: np.ndarray):
+    """Split the flat parameter vector into (W1 [256,64], b1, W2 [256,256], b2, w3, b3)."""
+    H, F = MLP_HIDDEN, MLP_FEATURES
+    o = 0
+    W1 = params[o:o + H * F].reshape(H, F); o += H * F
+    b1 = params[o:o + H]; o += H
+    W2 = params[o:o + H * H].reshape(H, H); o += H * H
+    b2 = params[o:o + H]; o += H
+    w3 = params[o:o + H]; o += H
+    b3 = params[o:o + 1]
+    return W1, b1, W2, b2, w3, b3
 
 
 def diag(prob: Problem, params: Params | None = None, want_rdm=False):
