@@ -42,6 +42,14 @@ struct Vec;
 template <bool kVec>
 struct Vec<float, 4, kVec> {
   float v[4];
+  __device__ __forceinline__ void store(float *p) const {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  // coherent load of data this kernel also writes
+  __device__ __forceinline__ void load_rw(const float *p) {
+    const float4 f = *reinterpret_cast<const float4 *>(p);
+    v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
+  }
   __device__ __forceinline__ void load(const float *p) {
     if (kVec) {
       const float4 f = __ldg(reinterpret_cast<const float4 *>(p));
@@ -55,6 +63,13 @@ struct Vec<float, 4, kVec> {
 template <bool kVec>
 struct Vec<double, 2, kVec> {
   double v[2];
+  __device__ __forceinline__ void store(double *p) const {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  }
+  __device__ __forceinline__ void load_rw(const double *p) {
+    const double2 f = *reinterpret_cast<const double2 *>(p);
+    v[0] = f.x, v[1] = f.y;
+  }
   __device__ __forceinline__ void load(const double *p) {
     if (kVec) {
       const double2 f = __ldg(reinterpret_cast<const double2 *>(p));
@@ -104,7 +119,7 @@ struct BlockArgs {
 //   beta pass: X = C^T.  Each thread adds its kBlkRows x VW results into
 //     sigma[Ia, Ib0 .. Ib0+kBlkRows) (contiguous along Ib) for its columns Ia.
 template <typename T, bool kAlpha, bool kVec>
-__global__ void __launch_bounds__(kBlkThreads, 1)
+__global__ void __launch_bounds__(kBlkThreads, 5)
     sigma_block_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
   constexpr int VW = 16 / sizeof(T);
   constexpr int W = kBlkThreads * VW;
@@ -213,37 +228,69 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
       }
     }
     if (kAlpha) {
+      // H_ii - shift: FP64 diagonal for the FP64 pass, (H_ii - H_00) in FP32 plus the FP64
+      // constant H_00 - shift for the FP32 pass
       const size_t idx = (size_t)row * ncols + cbase;
-      Vec<T, VW, kVec> xo;
+      const T *hsrc = sizeof(T) == 8 ? reinterpret_cast<const T *>(a.hii) : reinterpret_cast<const T *>(a.hii32);
+      const double hshift = sizeof(T) == 8 ? -a.core_shift : a.core_shift;
+      Vec<T, VW, kVec> xo, hv, ov;
       if (kVec && full) {
         xo.load(X + idx);
+        hv.load(hsrc + idx);
+        if (a.accumulate) ov.load_rw(out + idx);
       } else {
 #pragma unroll
-        for (int i = 0; i < VW; i++) xo.v[i] = ok[i] ? __ldg(X + idx + i) : T(0);
+        for (int i = 0; i < VW; i++) {
+          xo.v[i] = ok[i] ? __ldg(X + idx + i) : T(0);
+          hv.v[i] = ok[i] ? __ldg(hsrc + idx + i) : T(0);
+          ov.v[i] = (ok[i] && a.accumulate) ? out[idx + i] : T(0);
+        }
       }
 #pragma unroll
       for (int i = 0; i < VW; i++) {
         own[r][i] = xo.v[i];
-        if (!ok[i]) continue;
-        // H_ii - shift: FP64 diagonal for the FP64 pass, (H_ii - H_00) in FP32 plus the FP64
-        // constant H_00 - shift for the FP32 pass
-        const double hd = sizeof(T) == 8 ? __ldg(&a.hii[idx + i]) - a.core_shift
-                                         : (double)__ldg(&a.hii32[idx + i]) + a.core_shift;
-        double res = (double)acc[r][i] + hd * (double)xo.v[i];
-        if (a.accumulate) res += (double)out[idx + i];
-        out[idx + i] = (T)res;
+        double res = (double)acc[r][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+        if (a.accumulate) res += (double)ov.v[i];
+        ov.v[i] = (T)res;
+      }
+      if (kVec && full) {
+        ov.store(out + idx);
+      } else {
+#pragma unroll
+        for (int i = 0; i < VW; i++)
+          if (ok[i]) out[idx + i] = ov.v[i];
       }
     }
   }
-  // transposed write-out: column c gets rows r0 .. r0+nr contiguous (index c * nrows + r)
+  // transposed write-out: column c gets rows r0 .. r0+nr contiguous (index c * nrows + r), as
+  // 16-byte accesses when the block is full and every column starts 16-byte aligned
+  constexpr int RW = 16 / sizeof(T);
+  const bool vec_out = kVec && nr == kBlkRows && (a.nrows % RW) == 0;
 #pragma unroll
   for (int i = 0; i < VW; i++) {
+    if (!ok[i]) continue;
     const size_t o = (size_t)(cbase + i) * a.nrows + r0;
+    if (vec_out) {
 #pragma unroll
-    for (int r = 0; r < kBlkRows; r++) {
-      if (r < nr && ok[i]) {
-        if (kAlpha) XT[o + r] = own[r][i];
-        else out[o + r] += acc[r][i];
+      for (int r = 0; r < kBlkRows; r += RW) {
+        Vec<T, RW, true> v;
+        if (kAlpha) {
+#pragma unroll
+          for (int q = 0; q < RW; q++) v.v[q] = own[r + q][i];
+        } else {
+          v.load_rw(out + o + r);
+#pragma unroll
+          for (int q = 0; q < RW; q++) v.v[q] += acc[r + q][i];
+        }
+        v.store(kAlpha ? XT + o + r : out + o + r);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kBlkRows; r++) {
+        if (r < nr) {
+          if (kAlpha) XT[o + r] = own[r][i];
+          else out[o + r] += acc[r][i];
+        }
       }
     }
   }
@@ -373,7 +420,8 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
   // 16-byte column accesses need every row of X to start 16-byte aligned
   const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
-                   (!kAlpha || (ba.nrows % VW) == 0 || true);
+                   (reinterpret_cast<uintptr_t>(out) % 16) == 0 &&
+                   (!XT || (reinterpret_cast<uintptr_t>(XT) % 16) == 0);
   auto kern = vec ? sigma_block_kernel<T, kAlpha, true> : sigma_block_kernel<T, kAlpha, false>;
   TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
