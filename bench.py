@@ -120,6 +120,19 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def replica_throughput(pg, ms_local, dets_local, world, device="cpu"):
+    """Whole-job throughput of `world` replicas that each processed dets_local determinants in
+    ms_local device milliseconds: the slowest replica's time (all_reduce MAX) and the aggregate
+    GDets/s over it.  pg is torch.distributed (or None for one process)."""
+    import torch
+    ms_max = ms_local
+    if pg is not None:
+        t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+    return ms_max, world * dets_local / (ms_max * 1e-3) / 1e9
+
+
 def cpu_reference_sigma(prob_name, seconds_target, reps=1, threads=None):
     """Time the reference's CPU sigma (oracle/_ref/ref_bench) on the first `amax` alpha strings x
     all beta strings of the workload; amax is sized so the sample takes ~seconds_target."""
@@ -199,21 +212,34 @@ def end_to_end(h, x, N, dt, esz, world):
 
 
 def train_preconditioner(device):
-    """The learned preconditioner, trained on pairs from plain FP64 Davidson runs on the two
-    smaller configurations (12-orbital full CI, 24-orbital 4000 x 4000 selected CI)."""
+    """The learned preconditioner, trained on pairs from FP64 Davidson runs on the two smaller
+    configurations (12-orbital full CI, 24-orbital 4000 x 4000 selected CI): first along the
+    diagonal solver's trajectories, then two rounds along the learned solver's own trajectories
+    (each round adds its pairs and retrains)."""
     import sbd_tpb
     import synth
     t0 = time.perf_counter()
     pc = sbd_tpb.Precond(device, seed=2024)
-    for name, it in (("fci12", 4), ("sci24", 3)):
+    hs = []
+    for name in ("fci12", "sci24"):
         hh = sbd_tpb.Handle(device)
         hh.set_problem(synth.make_problem(name))
-        pc.collect(hh, sbd_tpb.default_params(max_it=it, max_nb=10, eps=1e-7), samples_per_step=1 << 16)
+        hs.append(hh)
+    t_collect = t_train = 0.0
+    for rnd in range(3):
+        tc = time.perf_counter()
+        for hh in hs:
+            pc.collect(hh, sbd_tpb.default_params(max_it=30, max_nb=10, eps=1e-8,
+                                                  preconditioner=0 if rnd == 0 else 1),
+                       samples_per_step=1 << 15)
+        t_collect += time.perf_counter() - tc
+        tt = time.perf_counter()
+        loss = pc.train(epochs=3 if rnd == 0 else 2, batch=8192, lr=1e-3)
+        t_train += time.perf_counter() - tt
+    for hh in hs:
         hh.close()
-    t_collect = time.perf_counter() - t0
-    loss = pc.train(epochs=4, batch=8192, lr=1e-3)
     lt, dt = pc.evaluate(0)
-    return pc, {"collect_s": t_collect, "train_s": time.perf_counter() - t0 - t_collect,
+    return pc, {"collect_s": t_collect, "train_s": t_train, "rounds": 3,
                 "pairs": pc.num_samples(0), "final_batch_loss": loss,
                 "train_error_learned_over_diagonal": lt / dt if dt > 0 else None}
 
@@ -300,13 +326,8 @@ def run_ours(args, world, rank, local, pg):
     ms_total = ev0.elapsed_time(ev1)
     launches = h.kernel_launches() - launches0
     barrier()
-    ms_max = ms_total
-    if pg is not None:
-        t = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max, value = replica_throughput(pg, ms_total, N * args.steps, world, device=f"cuda:{local}")
     ms_step = ms_max / args.steps
-    value = world * N * args.steps / (ms_max * 1e-3) / 1e9
 
     # per-kernel times of the same sigma (separate pass: reading them synchronises each call)
     kern = []

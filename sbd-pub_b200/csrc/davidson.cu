@@ -209,6 +209,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         }
         float *dk = nullptr;
         TPB_CUDA(cudaMalloc(&dk, sizeof(float) * n));
+        rec->owned.push_back(dk);
         rec->d.push_back(dk);
         TPB_CHECK((convert_vec<T, float>(h, tnext, dk, n)));
         rec->e0.push_back(ra.e0);
@@ -274,7 +275,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         if (recording) {
           float *dp = nullptr;
           TPB_CUDA(cudaMalloc(&dp, sizeof(float) * n));
-          rec->dperp.push_back(dp);
+          rec->owned.push_back(dp);
           TPB_CHECK((convert_vec<T, float>(h, tnext, dp, n)));
           rec->vec.push_back(dp);
           rec->scale.push_back(f[ib + 1]);
@@ -382,18 +383,15 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
 }
 
 int davidson_record(sbd_tpb_handle *h, const sbd_tpb_params *p, DavRecord *rec, double *Psi,
-                    double *energy) {
+                    double *energy, sbd_tpb_precond *learned) {
   if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "davidson: tables not built");
   if (p->max_nb < 2 || p->max_nb > kMaxSub)
     return fail(SBD_TPB_ERR_INVALID, "davidson: --block must be in [2, 16] for recording");
   if (p->max_it < 1) return fail(SBD_TPB_ERR_INVALID, "davidson: --iteration must be >= 1");
   double resid = 0.0;
   int nsig = 0, conv = 0;
-  TPB_CHECK(run_typed<double>(h, p, nullptr, 0.0, Psi, &resid, &nsig, &conv, rec, nullptr, energy, nullptr,
-                              nullptr));
-  // a step that ended the run (converged, or nothing left to add) has no dperp
-  while (rec->dperp.size() < rec->d.size()) rec->dperp.push_back(nullptr);
-  return SBD_TPB_OK;
+  return run_typed<double>(h, p, nullptr, 0.0, Psi, &resid, &nsig, &conv, rec, learned, energy, nullptr,
+                           nullptr);
 }
 
 }  // namespace sbdtpb

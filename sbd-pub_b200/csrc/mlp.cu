@@ -548,44 +548,55 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
 
 // ---------------------------------------------------------------- training pairs
 // A recorded step gives, per determinant i,
-//   a_i = d_i / |d|,   b_i = (d_i - dperp_i + alpha (P Psi)_i) / |d|,
-// with P Psi = Psi - sum_j g_j C_j the part of the converged vector outside the step's subspace
-// (g_j = C_j . Psi), dperp = P d (recorded after Gram-Schmidt) and alpha = (dperp . Psi) / |P Psi|^2
-// the scale that best fits P Psi to dperp.  Only the part of a correction outside the subspace
-// moves the Ritz vector, so b keeps d's in-subspace part (the network need not change it) and
-// replaces its outside part by the exact direction: (a - b) = (dperp - alpha P Psi) / |d| is the
-// diagonal correction's error, and the network is trained to shrink it.
+//   a_i = d_i / |d|,   b_i = (d_i - (Pd)_i + alpha (P Psi)_i) / |d|,
+// with P = 1 - sum_j C_j C_j^T the projector out of the step's subspace, Pd = d - sum_j hd_j vec_j
+// and P Psi = Psi - sum_j g_j vec_j, and alpha = (Pd . Psi) / |P Psi|^2 the scale that best fits
+// P Psi to Pd.  Only the part of a correction outside the subspace moves the Ritz vector, so b
+// keeps d's in-subspace part (the network need not change it) and replaces its outside part by the
+// exact direction: (a - b) = (Pd - alpha P Psi) / |d| is the diagonal correction's error, and the
+// network is trained to shrink it.
 constexpr int kMaxBasis = 16;
 
 struct PairArgs {
-  const float *d, *dperp;
+  const float *d;
   const double *Psi;
   const float *C[kMaxBasis];  // basis vectors (unnormalised)
-  double g[kMaxBasis];        // (C_j . Psi) * scale_j^2: P Psi = Psi - sum_j g_j vec_j
+  double g[kMaxBasis];        // P Psi = Psi - sum_j g_j C_j
+  double hd[kMaxBasis];       // P d   = d   - sum_j hd_j C_j
   int m;
   double inv_dn, alpha, c;    // 1/|d|, fit scale, sampling scale p = min(1, c (|a| + |b|))
   double e0, inv_rnorm;
   uint64_t seed;
 };
 
-__device__ __forceinline__ void pair_ab(const PairArgs &k, size_t i, double &A, double &B) {
-  double pp = k.Psi[i];
-  for (int j = 0; j < k.m; j++) pp -= k.g[j] * (double)k.C[j][i];
-  const double d = k.d[i];
-  A = d * k.inv_dn;
-  B = (d - (double)k.dperp[i] + k.alpha * pp) * k.inv_dn;
+__device__ __forceinline__ void pair_proj(const PairArgs &k, size_t i, double &d, double &pd, double &pp) {
+  d = k.d[i];
+  pd = d;
+  pp = k.Psi[i];
+  for (int j = 0; j < k.m; j++) {
+    const double c = k.C[j][i];
+    pd -= k.hd[j] * c;
+    pp -= k.g[j] * c;
+  }
 }
 
-// dots of a vector against Psi: partials[j * nblk + b] for j < nv (x_j . Psi)
-__global__ void psi_dots_kernel(PairArgs k, const double *__restrict__ Psi, size_t n, int nv,
-                                double *__restrict__ partials) {
-  double s[kMaxBasis + 1];
-  for (int j = 0; j <= kMaxBasis; j++) s[j] = 0.0;
+__device__ __forceinline__ void pair_ab(const PairArgs &k, size_t i, double &A, double &B) {
+  double d, pd, pp;
+  pair_proj(k, i, d, pd, pp);
+  A = d * k.inv_dn;
+  B = (d - pd + k.alpha * pp) * k.inv_dn;
+}
+
+// dots of the basis vectors against Psi (dsrc null) or against d: partials[j * nblk + b]
+__global__ void basis_dots_kernel(PairArgs k, const double *__restrict__ Psi, const float *__restrict__ dsrc,
+                                  size_t n, int nv, double *__restrict__ partials) {
+  double s[kMaxBasis];
+  for (int j = 0; j < kMaxBasis; j++) s[j] = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const double p = Psi[i];
+    const double p = dsrc ? (double)dsrc[i] : Psi[i];
     for (int j = 0; j < nv; j++) s[j] += (double)k.C[j][i] * p;
   }
-  __shared__ double red[kMaxBasis + 1][8];
+  __shared__ double red[kMaxBasis][8];
   for (int j = 0; j < nv; j++) {
     double v = s[j];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -599,17 +610,17 @@ __global__ void psi_dots_kernel(PairArgs k, const double *__restrict__ Psi, size
   }
 }
 
-// partials[0..3][b]: d.d, dperp.dperp, dperp.Psi, sum |a| + |b| (the last with k's coefficients)
+// partials[0..3][b]: d.d, Pd.Pd, Pd.Psi, sum |a| + |b| (the last with k's coefficients)
 __global__ void pair_sums_kernel(PairArgs k, size_t n, int with_ab, double *__restrict__ partials) {
   double s[4] = {0, 0, 0, 0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const double d = k.d[i], dp = k.dperp[i];
+    double d, pd, pp;
+    pair_proj(k, i, d, pd, pp);
     s[0] += d * d;
-    s[1] += dp * dp;
-    s[2] += dp * k.Psi[i];
+    s[1] += pd * pd;
+    s[2] += pd * k.Psi[i];
     if (with_ab) {
-      double A, B;
-      pair_ab(k, i, A, B);
+      const double A = d * k.inv_dn, B = (d - pd + k.alpha * pp) * k.inv_dn;
       s[3] += fabs(A) + fabs(B);
     }
   }
@@ -940,10 +951,9 @@ int add_step_pairs(sbd_tpb_precond *p, sbd_tpb_handle *h, const DavRecord &rec, 
   const size_t n = h->ndet();
   const int nblk = h->num_sms * 4;
   const std::vector<int> &bas = rec.basis[k];
-  if (!rec.dperp[k] || bas.empty() || (int)bas.size() > kMaxBasis) return SBD_TPB_OK;
+  if (bas.empty() || (int)bas.size() > kMaxBasis) return SBD_TPB_OK;
   PairArgs a{};
   a.d = rec.d[k];
-  a.dperp = rec.dperp[k];
   a.Psi = Psi;
   a.m = (int)bas.size();
   double g2 = 0.0;  // sum_j (C_j . Psi)^2
@@ -960,10 +970,23 @@ int add_step_pairs(sbd_tpb_precond *p, sbd_tpb_handle *h, const DavRecord &rec, 
   uint8_t *flags = nullptr;
   uint32_t *counts = nullptr;
   uint64_t *offs = nullptr;
-  TPB_CUDA(cudaMalloc(&part, sizeof(double) * (4 * (size_t)nblk + 8)));
-  double *res = part + 4 * (size_t)nblk;
+  TPB_CUDA(cudaMalloc(&part, sizeof(double) * ((kMaxBasis + 4) * (size_t)nblk + kMaxBasis + 4)));
+  double *res = part + (kMaxBasis + 4) * (size_t)nblk;
   int rc = SBD_TPB_OK;
   do {
+    // C_j . d for the projection of d
+    double cd[kMaxBasis];
+    basis_dots_kernel<<<nblk, 256, 0, h->stream>>>(a, Psi, a.d, n, a.m, part);
+    sum_partials_kernel<<<1, 32, 0, h->stream>>>(part, nblk, a.m, res);
+    if (cudaMemcpyAsync(cd, res, sizeof(double) * a.m, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      rc = fail(SBD_TPB_ERR_CUDA, "precond collect: basis dots");
+      break;
+    }
+    for (int j = 0; j < a.m; j++) {
+      const double sc = rec.scale[bas[j]];
+      a.hd[j] = sc * sc * cd[j];
+    }
     double sums[4];
     pair_sums_kernel<<<nblk, 256, 0, h->stream>>>(a, n, 0, part);
     sum_partials_kernel<<<1, 32, 0, h->stream>>>(part, nblk, 4, res);
@@ -972,10 +995,10 @@ int add_step_pairs(sbd_tpb_precond *p, sbd_tpb_handle *h, const DavRecord &rec, 
       rc = fail(SBD_TPB_ERR_CUDA, "precond collect: sums");
       break;
     }
-    const double dd = sums[0], dpdp = sums[1], dpPsi = sums[2], pp = 1.0 - g2;
-    if (!(dd > 0.0) || !(dpdp > 0.0) || !(pp > 1e-14)) break;  // nothing to learn from this step
+    const double dd = sums[0], pdpd = sums[1], pdPsi = sums[2], pp = 1.0 - g2;
+    if (!(dd > 0.0) || !(pdpd > 1e-30 * dd) || !(pp > 1e-14)) break;  // nothing to learn from this step
     a.inv_dn = 1.0 / std::sqrt(dd);
-    a.alpha = dpPsi / pp;
+    a.alpha = pdPsi / pp;
     pair_sums_kernel<<<nblk, 256, 0, h->stream>>>(a, n, 1, part);
     sum_partials_kernel<<<1, 32, 0, h->stream>>>(part, nblk, 4, res);
     if (cudaMemcpyAsync(sums, res, sizeof(sums), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
@@ -1033,14 +1056,14 @@ int basis_psi_dots(sbd_tpb_handle *h, const DavRecord &rec, const double *Psi, s
   const int nblk = h->num_sms * 4;
   out.assign(rec.vec.size(), 0.0);
   double *part = nullptr;
-  TPB_CUDA(cudaMalloc(&part, sizeof(double) * ((kMaxBasis + 1) * (size_t)nblk + kMaxBasis + 1)));
-  double *res = part + (kMaxBasis + 1) * (size_t)nblk;
+  TPB_CUDA(cudaMalloc(&part, sizeof(double) * (kMaxBasis * (size_t)nblk + kMaxBasis)));
+  double *res = part + kMaxBasis * (size_t)nblk;
   int rc = SBD_TPB_OK;
   for (size_t j0 = 0; j0 < rec.vec.size() && rc == SBD_TPB_OK; j0 += kMaxBasis) {
     const int nv = (int)std::min<size_t>(kMaxBasis, rec.vec.size() - j0);
     PairArgs a{};
     for (int j = 0; j < nv; j++) a.C[j] = rec.vec[j0 + j];
-    psi_dots_kernel<<<nblk, 256, 0, h->stream>>>(a, Psi, n, nv, part);
+    basis_dots_kernel<<<nblk, 256, 0, h->stream>>>(a, Psi, nullptr, n, nv, part);
     sum_partials_kernel<<<1, 32, 0, h->stream>>>(part, nblk, nv, res);
     if (cudaMemcpyAsync(out.data() + j0, res, sizeof(double) * nv, cudaMemcpyDeviceToHost, h->stream) !=
             cudaSuccess ||
@@ -1096,7 +1119,8 @@ int precond_collect(sbd_tpb_precond *p, sbd_tpb_handle *h, const sbd_tpb_params 
   double *Psi = nullptr;
   TPB_CUDA(cudaMalloc(&Psi, sizeof(double) * h->ndet()));
   double E = 0.0;
-  int rc = davidson_record(h, prm, &rec, Psi, &E);
+  // a run with the learned correction collects pairs along the learned solver's own trajectory
+  int rc = davidson_record(h, prm, &rec, Psi, &E, prm->preconditioner == SBD_TPB_PRECOND_LEARNED ? p : nullptr);
   std::vector<double> gpsi;
   if (rc == SBD_TPB_OK) rc = basis_psi_dots(h, rec, Psi, gpsi);
   for (size_t k = 0; rc == SBD_TPB_OK && k < rec.d.size(); k++)

@@ -11,33 +11,31 @@ constexpr int kMlpHidden = SBD_TPB_MLP_HIDDEN;   // width of both hidden layers
 constexpr int kMlpFeat = SBD_TPB_MLP_FEATURES;   // input width (K of the first layer)
 constexpr int kMlpWin = 24;                      // orbitals per spin around the Fermi level
 
-// Steps of a plain FP64 Davidson run kept for training (FP32 copies, separated convention).
-// Step k: the diagonal correction d_k = r_k / (E_k - H_ii), its part orthogonal to the step's
-// subspace dperp_k (what Gram-Schmidt keeps), E_k, |r_k| and the indices of its orthonormal basis
-// vectors C_j = scale_j * vec_j.  A basis vector is either a cycle's start vector or the dperp of
-// an earlier step.
+// Steps of a Davidson run kept for training (FP32 copies, separated convention).  Step k: the
+// diagonal correction d_k = r_k / (E_k - H_ii), E_k, |r_k| and the indices of its orthonormal
+// basis vectors C_j = scale_j * vec_j (a cycle's start vector, then the Gram-Schmidt images of
+// the corrections actually added).  The run may use the learned correction, so pairs can be
+// collected along the learned solver's own trajectory.
 struct DavRecord {
-  std::vector<float *> d, dperp;
+  std::vector<float *> d;
   std::vector<double> e0, rnorm;
   std::vector<std::vector<int>> basis;  // per step: indices into vec/scale
   std::vector<const float *> vec;       // basis vectors (owned through owned)
   std::vector<double> scale;
-  std::vector<float *> owned;           // cycle start vectors
+  std::vector<float *> owned;
   int max_steps = 64;
   DavRecord() = default;
   DavRecord(const DavRecord &) = delete;
   DavRecord &operator=(const DavRecord &) = delete;
   ~DavRecord() {
-    for (float *p : d) cudaFree(p);
-    for (float *p : dperp) cudaFree(p);
     for (float *p : owned) cudaFree(p);
   }
 };
 
-// Plain FP64 diagonal Davidson with recording; Psi (device, n doubles) receives the normalised
-// final vector, energy the last Ritz value.
+// FP64 Davidson with recording (diagonal correction, or the learned one when learned is given);
+// Psi (device, n doubles) receives the normalised final vector, energy the last Ritz value.
 int davidson_record(sbd_tpb_handle *h, const sbd_tpb_params *p, DavRecord *rec, double *Psi,
-                    double *energy);
+                    double *energy, sbd_tpb_precond *learned);
 
 // t[i] <- t[i] * (1 + y_i) in place, t holding the diagonal correction of Ritz value e0 and
 // residual norm rnorm on the handle's stream.

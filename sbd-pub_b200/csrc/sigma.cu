@@ -16,6 +16,7 @@
 // The alpha-beta term of FCI-like problems (dense singles) goes through the gather -> dense
 // (pq|rs) contraction -> scatter path in ab_dense.cu instead of the direct loop.
 #include <algorithm>
+#include <string>
 
 #include "tpb_common.cuh"
 
@@ -306,12 +307,11 @@ __global__ void __launch_bounds__(kBlkThreads, 5)
 // false) the same loop reads C and the integrals through L1/L2.
 struct AbSparseArgs {
   const uint32_t *rows;  // alpha rows with at least one single
-  const uint32_t *cols;  // beta columns with at least one single (ascending)
+  const uint2 *colp;     // beta columns with singles: (column, first entry), then (0, nnz)
+  const uint2 *bsp;      // beta singles entries: (ket, +-(rs + 1) with the beta sign)
   uint32_t ncols_s;
   const uint32_t *as_off, *as_ket;
   const int32_t *as_pair;  // +-(pq + 1), sign = alpha sign
-  const uint32_t *bs_off, *bs_ket;
-  const int32_t *bs_pair;  // +-(rs + 1), sign = beta sign
   const double *eri;       // (pq|rs) [L*L][L*L]
   int L2;
   uint32_t nb;     // row length of C and sigma
@@ -346,12 +346,13 @@ __global__ void __launch_bounds__(256)
       __syncthreads();
     }
     for (uint32_t q = threadIdx.x; q < a.ncols_s; q += blockDim.x) {
-      const uint32_t ib = __ldg(&a.cols[q]);
-      const uint32_t f0 = __ldg(&a.bs_off[ib]), f1 = __ldg(&a.bs_off[ib + 1]);
+      const uint2 c0 = __ldg(&a.colp[q]), c1 = __ldg(&a.colp[q + 1]);
+      const uint32_t ib = c0.x;
       double acc = 0.0;
-      for (uint32_t f = f0; f < f1; f++) {
-        const uint32_t jb = __ldg(&a.bs_ket[f]);
-        const int32_t pb = __ldg(&a.bs_pair[f]);
+      for (uint32_t f = c0.y; f < c1.y; f++) {
+        const uint2 be = __ldg(&a.bsp[f]);
+        const uint32_t jb = be.x;
+        const int32_t pb = (int32_t)be.y;
         const int rs = (pb > 0 ? pb : -pb) - 1;
         double sum = 0.0;
         for (uint32_t j = 0; j < ng; j++) {
@@ -453,7 +454,7 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
     h->blk_for = h->ta_d.ket;
   }
   if (want_ab_lists && !h->d_ab_rows && na > 0 && nb > 0) {
-    std::vector<uint32_t> ao(na + 1), bo(nb + 1), rows, cols;
+    std::vector<uint32_t> ao(na + 1), bo(nb + 1), rows;
     TPB_CUDA(cudaMemcpy(ao.data(), h->ta_s.off, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToHost));
     TPB_CUDA(cudaMemcpy(bo.data(), h->tb_s.off, sizeof(uint32_t) * (nb + 1), cudaMemcpyDeviceToHost));
     uint32_t kmax = 0;
@@ -462,16 +463,30 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
         rows.push_back((uint32_t)i);
         kmax = std::max(kmax, ao[i + 1] - ao[i]);
       }
+    // beta program: columns with singles and their entries, packed so a thread needs one load
+    // per column and one per entry
+    const size_t nnz = bo[nb];
+    std::vector<uint32_t> bket(std::max<size_t>(1, nnz));
+    std::vector<int32_t> bpair(std::max<size_t>(1, nnz));
+    if (nnz) {
+      TPB_CUDA(cudaMemcpy(bket.data(), h->tb_s.ket, sizeof(uint32_t) * nnz, cudaMemcpyDeviceToHost));
+      TPB_CUDA(cudaMemcpy(bpair.data(), h->pb.s_pair, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
+    }
+    std::vector<uint2> colp, bsp(std::max<size_t>(1, nnz));
     for (size_t i = 0; i < nb; i++)
-      if (bo[i + 1] > bo[i]) cols.push_back((uint32_t)i);
+      if (bo[i + 1] > bo[i]) colp.push_back(make_uint2((uint32_t)i, bo[i]));
+    const size_t ncs = colp.size();
+    colp.push_back(make_uint2(0u, (uint32_t)nnz));
+    for (size_t f = 0; f < nnz; f++) bsp[f] = make_uint2(bket[f], (uint32_t)bpair[f]);
     TPB_CUDA(cudaMalloc(&h->d_ab_rows, sizeof(uint32_t) * std::max<size_t>(1, rows.size())));
-    TPB_CUDA(cudaMalloc(&h->d_ab_cols, sizeof(uint32_t) * std::max<size_t>(1, cols.size())));
+    TPB_CUDA(cudaMalloc(&h->d_ab_colp, sizeof(uint2) * colp.size()));
+    TPB_CUDA(cudaMalloc(&h->d_ab_bsp, sizeof(uint2) * bsp.size()));
     if (!rows.empty())
       TPB_CUDA(cudaMemcpy(h->d_ab_rows, rows.data(), sizeof(uint32_t) * rows.size(), cudaMemcpyHostToDevice));
-    if (!cols.empty())
-      TPB_CUDA(cudaMemcpy(h->d_ab_cols, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice));
+    TPB_CUDA(cudaMemcpy(h->d_ab_colp, colp.data(), sizeof(uint2) * colp.size(), cudaMemcpyHostToDevice));
+    TPB_CUDA(cudaMemcpy(h->d_ab_bsp, bsp.data(), sizeof(uint2) * bsp.size(), cudaMemcpyHostToDevice));
     h->ab_nrows = (uint32_t)rows.size();
-    h->ab_ncols = (uint32_t)cols.size();
+    h->ab_ncols = (uint32_t)ncs;
     h->ab_max_k = kmax;
   }
   return SBD_TPB_OK;
@@ -482,14 +497,12 @@ int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
   if (h->ab_nrows == 0 || h->ab_ncols == 0) return SBD_TPB_OK;
   AbSparseArgs a{};
   a.rows = h->d_ab_rows;
-  a.cols = h->d_ab_cols;
+  a.colp = h->d_ab_colp;
+  a.bsp = h->d_ab_bsp;
   a.ncols_s = h->ab_ncols;
   a.as_off = h->ta_s.off;
   a.as_ket = h->ta_s.ket;
   a.as_pair = h->pa.s_pair;
-  a.bs_off = h->tb_s.off;
-  a.bs_ket = h->tb_s.ket;
-  a.bs_pair = h->pb.s_pair;
   a.eri = h->d_eri;
   a.L2 = h->L * h->L;
   a.nb = (uint32_t)h->bstr.size();

@@ -77,6 +77,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
 // 1-D bulk copy global -> shared (this CTA), completion counted on mbar
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
   asm volatile(

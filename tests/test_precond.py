@@ -193,6 +193,14 @@ def trained():
     before = pc.evaluate(0)
     held_before = pc.evaluate(1)
     loss = pc.train(epochs=4, batch=8192, lr=1e-3)
+    # one more round on pairs from the learned solver's own trajectory
+    h = sbd_tpb.Handle(0)
+    h.set_problem(synth.make_problem("fci12"))
+    pc.collect(h, sbd_tpb.default_params(max_it=30, max_nb=10, eps=1e-8,
+                                         preconditioner=sbd_tpb.PRECOND_LEARNED),
+               samples_per_step=1 << 15, role=0)
+    h.close()
+    loss = pc.train(epochs=2, batch=8192, lr=1e-3)
     return dict(pc=pc, e_train=e_train, before=before, held_before=held_before, loss=loss)
 
 
