@@ -351,9 +351,16 @@ def run_ours(args, world, rank, local, pg):
     dom = int(np.argmax(kern))
     pk = peaks()
     achieved = per[dom] / (kern[dom] * 1e-3) / 1e9
+    # DRAM bytes per determinant of each pass from the ncu capture at 10^8 determinants (FP32,
+    # profiles/sigma_kernels_sci28_fp32.md), scaled to this workload's determinants
+    traffic_per_det = {"sigma_block_kernel<alpha>": 18.05, "sigma_block_kernel<beta>": 12.96}
+    traffic = (traffic_per_det[names[dom]] * N / 1e9
+               if dt == torch.float32 and names[dom] in traffic_per_det else None)
     roofline = {"kernel": names[dom], "bound": "hbm", "achieved": achieved,
                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
-                "traffic": None, "peak_source": "measured" if not pk.get("fallback") else "fallback",
+                "traffic": traffic, "traffic_unit": "GB per launch",
+                "traffic_source": "ncu capture at 1e8 determinants scaled by determinants" if traffic else None,
+                "peak_source": "measured" if not pk.get("fallback") else "fallback",
                 "kernel_ms": {names[i]: float(kern[i]) for i in range(len(kern))},
                 "algorithmic_bytes": {names[i]: int(per[i]) for i in range(len(kern))}}
 

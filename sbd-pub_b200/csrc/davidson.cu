@@ -223,6 +223,11 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         const bool failed = ib > 0 && prev_learned && !(norm_R < prev_norm);
         use_learned = !failed;
         if (failed) nfallback++;
+        // a network that keeps failing on this problem is switched off for the rest of the solve
+        if (nlearned >= 8 && 3 * nfallback > nlearned) {
+          learned = nullptr;
+          use_learned = false;
+        }
       }
       prev_learned = use_learned;
       prev_norm = norm_R;
@@ -237,7 +242,8 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         stop = true;
         break;
       }
-      if (use_learned) TPB_CHECK(precond_apply<T>(h, learned, tnext, ra.e0, std::sqrt(out[1])));
+      if (use_learned)
+        TPB_CHECK(precond_apply<T>(h, learned, tnext, ra.e0, std::sqrt(out[1]), out[2 + ib + 1]));
       if (sym && !last) {
         // the S_k are exactly symmetric, so S_k.t is unchanged by the projection; only t.t is
         TPB_CHECK(symmetrize<T>(h, tnext, &out[2 + ib + 1]));

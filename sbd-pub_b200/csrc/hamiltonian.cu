@@ -191,6 +191,7 @@ void free_device_problem(sbd_tpb_handle *h) {
   if (h->d_ct) cudaFree(h->d_ct);
   h->d_ct = nullptr;
   h->ct_bytes = 0;
+  free_dev(h->d_mlp_idx);
   free_dev(h->d_occw_a);
   free_dev(h->d_occw_b);
   free_dev(h->d_ab_rows);

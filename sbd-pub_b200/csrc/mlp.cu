@@ -391,7 +391,8 @@ struct InferArgs {
   double e0, inv_rnorm;
   const uint32_t *occ_a, *occ_b;
   uint32_t nb;
-  size_t n;
+  const uint32_t *idx;  // determinants to correct (null: all of 0 .. count-1)
+  size_t count;
   const bf16 *W1p, *W2p;
   const float *P;
   int *err;
@@ -435,18 +436,20 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
   }
   __syncthreads();
 
-  const size_t ntiles = (a.n + 127) / 128;
+  const size_t ntiles = (a.count + 127) / 128;
   const int row = quad * 32 + lane;  // TMEM lane of this thread in the epilogues
   const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
   for (size_t tile = blockIdx.x; tile < ntiles && *status == 0; tile += gridDim.x) {
     // features of the tile's 128 determinants (threads 0..127, one row each)
     if (threadIdx.x < 128) {
       const int r = threadIdx.x;
-      const size_t i = tile * 128 + r;
+      const size_t kk = tile * 128 + r;
+      const bool live = kk < a.count;
+      const size_t i = live ? (a.idx ? (size_t)__ldg(&a.idx[kk]) : kk) : 0;
       float fe = 0.f, fr = 0.f;
       uint32_t oa = 0, ob = 0;
       double d = 0.0;
-      if (i < a.n) {
+      if (live) {
         d = (double)t[i];
         const double hd = __ldg(&a.hii[i]);
         cont_features(d, hd, a.e0, a.inv_rnorm, fe, fr);
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
       dsh[r] = d;
 #pragma unroll
       for (int g = 0; g < F / 8; g++) {
-        const uint4 u = (i < a.n) ? feature_group(g, fe, fr, oa, ob) : make_uint4(0, 0, 0, 0);
+        const uint4 u = live ? feature_group(g, fe, fr, oa, ob) : make_uint4(0, 0, 0, 0);
         *reinterpret_cast<uint4 *>(sA + a_off((size_t)r, g * 8, F) * 2) = u;
       }
       fence_proxy_async();
@@ -534,8 +537,9 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
     fence_before_sync();
     __syncthreads();
     if (half == 0) {
-      const size_t i = tile * 128 + row;
-      if (i < a.n) {
+      const size_t kk = tile * 128 + row;
+      if (kk < a.count) {
+        const size_t i = a.idx ? (size_t)__ldg(&a.idx[kk]) : kk;
         const float y = acc + part[row] + __ldg(&a.P[ob3]);
         t[i] = (T)(dsh[row] * (1.0 + (double)y));
       }
@@ -544,6 +548,20 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
   }
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// Determinants whose diagonal correction is at least theta in magnitude, compacted into idx (order
+// arbitrary: every corrected entry depends only on itself).  With theta = |d| / sqrt(cap) at most
+// cap entries qualify (sum of d_i^2 over them is at most |d|^2); the counter guards the rest.
+template <typename T>
+__global__ void select_kernel(const T *__restrict__ d, size_t n, double theta, uint32_t *__restrict__ idx,
+                              uint32_t cap, unsigned long long *__restrict__ count) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (fabs((double)d[i]) >= theta) {
+      const unsigned long long pos = atomicAdd(count, 1ull);
+      if (pos < cap) idx[pos] = (uint32_t)i;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- training pairs
@@ -1077,7 +1095,7 @@ int basis_psi_dots(sbd_tpb_handle *h, const DavRecord &rec, const double *Psi, s
 }  // namespace
 
 template <typename T>
-int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double rnorm) {
+int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double rnorm, double tt) {
   TPB_CHECK(ensure_occ_windows(h));
   InferArgs a{};
   a.hii = h->d_hii;
@@ -1086,14 +1104,33 @@ int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double
   a.occ_a = h->d_occw_a;
   a.occ_b = h->d_occw_b;
   a.nb = (uint32_t)h->bstr.size();
-  a.n = h->ndet();
+  const size_t n = h->ndet();
+  a.idx = nullptr;
+  a.count = n;
+  if (n > kMlpBudget && tt > 0.0 && n < ((size_t)1 << 32)) {
+    // correct only the entries that carry the correction: |d_i| >= |d| / sqrt(budget)
+    if (!h->d_mlp_idx) {
+      TPB_CUDA(cudaMalloc(&h->d_mlp_idx, sizeof(uint32_t) * kMlpBudget + sizeof(unsigned long long)));
+    }
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(h->d_mlp_idx + kMlpBudget);
+    TPB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), h->stream));
+    select_kernel<T><<<h->num_sms * 8, 256, 0, h->stream>>>(t, n, std::sqrt(tt / (double)kMlpBudget),
+                                                            h->d_mlp_idx, (uint32_t)kMlpBudget, cnt);
+    TPB_LAUNCHED(h);
+    unsigned long long c = 0;
+    TPB_CUDA(cudaMemcpyAsync(&c, cnt, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    TPB_CUDA(cudaStreamSynchronize(h->stream));
+    a.idx = h->d_mlp_idx;
+    a.count = (size_t)std::min<unsigned long long>(c, kMlpBudget);
+    if (a.count == 0) return SBD_TPB_OK;
+  }
   a.W1p = p->W1p;
   a.W2p = p->W2p;
   a.P = p->P;
   a.err = p->err;
   if (kSmInfer > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "learned preconditioner: shared memory");
   TPB_CUDA(cudaFuncSetAttribute(mlp_infer_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmInfer));
-  const size_t ntiles = (a.n + 127) / 128;
+  const size_t ntiles = (a.count + 127) / 128;
   const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)h->num_sms);
   // the weights may have been written on the preconditioner's stream
   TPB_CUDA(cudaStreamSynchronize(p->stream));
@@ -1109,8 +1146,8 @@ int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double
   return SBD_TPB_OK;
 }
 
-template int precond_apply<double>(sbd_tpb_handle *, sbd_tpb_precond *, double *, double, double);
-template int precond_apply<float>(sbd_tpb_handle *, sbd_tpb_precond *, float *, double, double);
+template int precond_apply<double>(sbd_tpb_handle *, sbd_tpb_precond *, double *, double, double, double);
+template int precond_apply<float>(sbd_tpb_handle *, sbd_tpb_precond *, float *, double, double, double);
 
 int precond_collect(sbd_tpb_precond *p, sbd_tpb_handle *h, const sbd_tpb_params *prm, size_t samples, int role,
                     double *energy) {
@@ -1365,7 +1402,7 @@ extern "C" int sbd_tpb_precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, cons
   int rc = SBD_TPB_OK;
   if (cudaMemcpyAsync(dv, d, n * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
     rc = fail(SBD_TPB_ERR_CUDA, "precond apply: upload");
-  if (rc == SBD_TPB_OK) rc = precond_apply<double>(h, p, dv, e0, rnorm);
+  if (rc == SBD_TPB_OK) rc = precond_apply<double>(h, p, dv, e0, rnorm, 0.0);
   if (rc == SBD_TPB_OK && (cudaMemcpyAsync(t, dv, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
                            cudaStreamSynchronize(h->stream) != cudaSuccess))
     rc = fail(SBD_TPB_ERR_CUDA, "precond apply: download");

@@ -37,10 +37,14 @@ struct DavRecord {
 int davidson_record(sbd_tpb_handle *h, const sbd_tpb_params *p, DavRecord *rec, double *Psi,
                     double *energy, sbd_tpb_precond *learned);
 
+// Most determinants the network corrects per application; beyond it only the entries with
+// |d_i| >= |d| / sqrt(budget) are corrected (the others keep the diagonal correction).
+constexpr size_t kMlpBudget = (size_t)1 << 22;
+
 // t[i] <- t[i] * (1 + y_i) in place, t holding the diagonal correction of Ritz value e0 and
-// residual norm rnorm on the handle's stream.
+// residual norm rnorm (tt = t.t, 0 = correct every entry) on the handle's stream.
 template <typename T>
-int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double rnorm);
+int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double rnorm, double tt);
 
 // Occupation window of one string: bit q = occupation of orbital nel - 12 + q (1 below orbital 0).
 __host__ __device__ inline uint32_t occ_window(uint64_t s, int nel) {
