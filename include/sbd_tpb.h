@@ -239,7 +239,9 @@ SBD_TPB_API int sbd_tpb_precond_gradients(sbd_tpb_precond *p, size_t n, const fl
                                           const float *b, const float *w, float *grad, double *loss,
                                           float *y);
 /* The fused inference kernel on the handle's determinants: t = d (1 + y) from d (host, FP64,
- * separated convention, [na*nb]), E0 and |r|.  For parity tests. */
+ * separated convention, [na*nb]), E0 and |r|.  Beyond 2^22 determinants only the entries with
+ * |d_i| >= |d| / 2^11 are corrected (at most 2^22 of them), as inside the Davidson loop; the
+ * others keep t_i = d_i.  For parity tests. */
 SBD_TPB_API int sbd_tpb_precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, const double *d, double e0,
                                       double rnorm, double *t);
 /* Attaches p (or NULL) to the handle: Davidson with preconditioner SBD_TPB_PRECOND_LEARNED uses

@@ -1402,7 +1402,9 @@ extern "C" int sbd_tpb_precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, cons
   int rc = SBD_TPB_OK;
   if (cudaMemcpyAsync(dv, d, n * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
     rc = fail(SBD_TPB_ERR_CUDA, "precond apply: upload");
-  if (rc == SBD_TPB_OK) rc = precond_apply<double>(h, p, dv, e0, rnorm, 0.0);
+  double tt = 0.0;  // |d|^2: beyond the budget only the large entries are corrected
+  for (size_t i = 0; i < n; i++) tt += d[i] * d[i];
+  if (rc == SBD_TPB_OK) rc = precond_apply<double>(h, p, dv, e0, rnorm, tt);
   if (rc == SBD_TPB_OK && (cudaMemcpyAsync(t, dv, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
                            cudaStreamSynchronize(h->stream) != cudaSuccess))
     rc = fail(SBD_TPB_ERR_CUDA, "precond apply: download");

@@ -173,6 +173,43 @@ def test_gpu_mlp_inference_kernel_vs_oracle():
     h.close()
 
 
+@pytest.mark.gpu
+def test_gpu_mlp_inference_budgeted_subset():
+    """Beyond 2^22 determinants the inference kernel corrects only |d_i| >= |d| / 2^11 (gathered by
+    index); the other entries keep the diagonal correction exactly."""
+    import sbd_tpb
+    import synth
+    prob = synth.make_problem("sci24")  # 16M determinants
+    h = sbd_tpb.Handle(0)
+    h.set_problem(prob)
+    rng = np.random.default_rng(8)
+    P = random_params(rng, scale3=0.5)
+    pc = sbd_tpb.Precond(0, seed=5)
+    pc.set_params(flat(P))
+    n = prob.ndet
+    hd = h.diagonal()
+    d = rng.standard_cauchy(size=n) * 1e-3  # heavy-tailed: a few large entries
+    e0, rnorm = float(hd.min()) - 0.2, 1.3
+    t = pc.apply(h, d, e0, rnorm)
+    theta = np.sqrt(np.dot(d, d) / (1 << 22))
+    big = np.abs(d) >= theta * (1 + 1e-9)       # away from the threshold on both sides: the
+    small = np.abs(d) < theta * (1 - 1e-9)      # library sums |d|^2 in another order
+    assert 0 < big.sum() <= (1 << 22)
+    assert np.array_equal(t[small], d[small])
+    # the corrected entries agree with the training forward pass on the same features
+    sel = np.flatnonzero(big)[:2048]
+    nb = len(prob.bstr)
+    nel = bin(int(prob.astr[0])).count("1")
+    wa = np.array([occ_window(prob.astr[i // nb], nel) for i in sel])
+    wb = np.array([occ_window(prob.bstr[i % nb], nel) for i in sel])
+    x = features(d[sel], hd[sel], e0, rnorm, wa, wb)
+    one = np.ones(len(sel), np.float32)
+    _, _, y_train = pc.gradients(bf16(x), one, one, one)
+    y_gpu = t[sel] / d[sel] - 1.0
+    assert np.max(np.abs(y_gpu - y_train)) < 1e-2 * (1 + np.max(np.abs(y_train)))
+    h.close()
+
+
 @pytest.fixture(scope="module")
 def trained():
     """A preconditioner trained on pairs of the plain FP64 Davidson on the 12-orbital full CI
