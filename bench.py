@@ -46,7 +46,26 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
+    ap.add_argument("--davidson-cycle", action="store_true",
+                    help="only run one Davidson cycle (8 sigma steps, final FP64 sigma) on the workload "
+                         "and print its time; the command the Davidson launch-list profile is taken on")
     return ap.parse_args()
+
+
+def run_davidson_cycle(args, local):
+    import sbd_tpb
+    import synth
+    prob = synth.make_problem(args.workload)
+    h = sbd_tpb.Handle(local)
+    h.set_problem(prob)
+    prec = sbd_tpb.MIXED if args.precision == "mixed" else sbd_tpb.FP64
+    t0 = time.perf_counter()
+    r = h.davidson(sbd_tpb.default_params(max_it=1, max_nb=8, eps=1e-12, precision=prec), want_vector=False)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"workload": args.workload, "precision": args.precision, "sigma_steps": r["iterations"],
+                      "seconds": dt, "ms_per_step": 1e3 * dt / max(1, r["iterations"]),
+                      "energy": r["energy"]}), flush=True)
+    h.close()
 
 
 def peaks():
@@ -409,6 +428,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.davidson_cycle:
+            run_davidson_cycle(args, local)
         else:
             run_ours(args, world, rank, local, pg)
     finally:
