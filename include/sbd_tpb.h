@@ -112,6 +112,12 @@ SBD_TPB_API int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamilto
                  const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
                  sbd_tpb_result *result);
 
+/* Same, starting Davidson from W0 (host, [na*nb], reference convention and order; NULL = the HF
+ * start) -- the reference's --loadname restart (tpb/sbdiag.h:280-291). */
+SBD_TPB_API int sbd_tpb_diag_from(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
+                                  const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                                  const double *W0, sbd_tpb_result *result);
+
 /* ---- handle API: the stages of the same path, for callers that drive them ---------------- */
 SBD_TPB_API const char *sbd_tpb_last_error(void);
 SBD_TPB_API int sbd_tpb_create(int device, sbd_tpb_handle **out);
@@ -204,10 +210,14 @@ SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);
  *   t_i = d_i * (1 + y_i),  d_i = r_i / (E0 - H_ii),
  *   y = w3 . gelu(W2 gelu(W1 x + b1) + b2) + b3   (hidden width 256, tanh-form GELU, BF16
  *   weights and activations on tensor cores, FP32 accumulation),
- * with x = [asinh(H_ii - E0)/4, asinh(1e4 r_i/|r|)/10, the occupations of the 24 alpha and 24
- * beta orbitals n-12 .. n+11 around the Fermi level (orbitals below 0 read as occupied), 14
- * zeros].  It is trained by the library's own forward/backward kernels on pairs (d_k, exact
- * correction Psi - W_k) recorded from plain FP64 Davidson runs; w3 = b3 = 0 at creation, so an
+ * with x = [asinh(E_J - E0)/4, 0, which of the 24 orbitals n-12 .. n+11 around the Fermi level
+ * are doubly occupied, which singly, 14 zeros] (orbitals below 0 read as occupied; n = electrons
+ * per spin); E_J is the spin-free diagonal, H_ii plus the same-spin exchange integrals of both
+ * strings.  The inputs depend only on the spatial occupation, so every determinant of a
+ * spin-coupled set gets the same factor and the learned correction keeps the spin symmetry the
+ * diagonal one keeps (the residual entry r_i, which differs within such a set, is left out: its
+ * input slot is zero).  It is trained by the library's own forward/backward kernels on pairs
+ * (d_k, exact correction) recorded from FP64 Davidson runs; w3 = b3 = 0 at creation, so an
  * untrained network is exactly the diagonal preconditioner.  The parameter vector is FP32 in
  * the order W1[256][64], b1[256], W2[256][256], b2[256], w3[256], b3. */
 typedef struct sbd_tpb_precond sbd_tpb_precond;

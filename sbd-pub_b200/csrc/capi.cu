@@ -359,6 +359,12 @@ int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, in
 int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
                  const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
                  sbd_tpb_result *result) {
+  return sbd_tpb_diag_from(params, ham, astr, na, bstr, nb, nullptr, result);
+}
+
+int sbd_tpb_diag_from(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
+                      const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                      const double *W0, sbd_tpb_result *result) {
   if (!params || !result) return fail(SBD_TPB_ERR_INVALID, "null params/result");
   const auto t0 = std::chrono::steady_clock::now();
   sbd_tpb_handle *h = nullptr;
@@ -376,7 +382,7 @@ int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,
       result->one_rdm = nullptr;
       result->two_rdm = nullptr;
     }
-    rc = sbd_tpb_davidson(h, params, nullptr, result);
+    rc = sbd_tpb_davidson(h, params, W0, result);
     result->one_rdm = one;
     result->two_rdm = two;
   }

@@ -192,6 +192,8 @@ void free_device_problem(sbd_tpb_handle *h) {
   h->d_ct = nullptr;
   h->ct_bytes = 0;
   free_dev(h->d_mlp_idx);
+  free_dev(h->d_kx_a);
+  free_dev(h->d_kx_b);
   free_dev(h->d_occw_a);
   free_dev(h->d_occw_b);
   free_dev(h->d_ab_rows);

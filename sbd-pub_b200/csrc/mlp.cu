@@ -63,30 +63,34 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * 0.7978845608028654f * (1.f + 0.134145f * z * z);
 }
 
-// the two continuous features of a determinant from its diagonal correction d
-__device__ __forceinline__ void cont_features(double d, double hd, double e0, double inv_rnorm, float &fe,
-                                              float &fr) {
-  double den = e0 - hd;
-  if (!(fabs(den) > 1.0e-12)) den -= 1.0e-12;  // the residual kernel's regularisation
-  const double r = d * den;
-  fe = asinhf((float)(hd - e0)) * 0.25f;
-  fr = asinhf((float)(r * inv_rnorm * 1.0e4)) * 0.1f;
+// Features depend only on a determinant's spatial occupation (which orbitals are empty, singly or
+// doubly occupied), never on which singly occupied orbitals carry alpha and which beta.  Every
+// determinant of a spin-coupled set then gets the same factor 1 + y, so the learned correction
+// (1 + Y) D r commutes with S^2 wherever the diagonal one D r does, and cannot steer the solver to a
+// state of another spin than the diagonal correction's: the energy feature is the spin-free diagonal
+// E_J = H_ii + sum of the same-spin exchange integrals of both strings (Coulomb terms only), and
+// the residual-entry input is held at zero (r_i differs within a spin-coupled set).
+__device__ __forceinline__ void cont_features(double hdJ, double e0, float &fe, float &fr) {
+  fe = asinhf((float)(hdJ - e0)) * 0.25f;
+  fr = 0.f;
 }
 
-// 8 consecutive features k0..k0+7 of one row as BF16
+// 8 consecutive features k0..k0+7 of one row as BF16: [fe, fr, doubly occupied window (24),
+// singly occupied window (24), 14 zeros]
 __device__ __forceinline__ uint4 feature_group(int g, float fe, float fr, uint32_t oa, uint32_t ob) {
   union {
     bf16 h[8];
     uint4 u;
   } o;
+  const uint32_t dbl = oa & ob, sgl = oa ^ ob;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     const int k = g * 8 + i;
     float x = 0.f;
     if (k == 0) x = fe;
     else if (k == 1) x = fr;
-    else if (k < 2 + kMlpWin) x = (float)((oa >> (k - 2)) & 1u);
-    else if (k < 2 + 2 * kMlpWin) x = (float)((ob >> (k - 2 - kMlpWin)) & 1u);
+    else if (k < 2 + kMlpWin) x = (float)((dbl >> (k - 2)) & 1u);
+    else if (k < 2 + 2 * kMlpWin) x = (float)((sgl >> (k - 2 - kMlpWin)) & 1u);
     o.h[i] = __float2bfloat16_rn(x);
   }
   return o.u;
@@ -388,6 +392,7 @@ constexpr uint32_t kSmInfer = kSmW1 + kSmW2 + kSmA + kSmPart + kSmD + 64;
 
 struct InferArgs {
   const double *hii;
+  const double *kxa, *kxb;  // same-spin exchange sums of the alpha / beta strings
   double e0, inv_rnorm;
   const uint32_t *occ_a, *occ_b;
   uint32_t nb;
@@ -451,11 +456,10 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
       double d = 0.0;
       if (live) {
         d = (double)t[i];
-        const double hd = __ldg(&a.hii[i]);
-        cont_features(d, hd, a.e0, a.inv_rnorm, fe, fr);
-        const size_t ia = i / a.nb;
+        const size_t ia = i / a.nb, ib = i - ia * a.nb;
+        cont_features(__ldg(&a.hii[i]) + __ldg(&a.kxa[ia]) + __ldg(&a.kxb[ib]), a.e0, fe, fr);
         oa = __ldg(&a.occ_a[ia]);
-        ob = __ldg(&a.occ_b[i - ia * a.nb]);
+        ob = __ldg(&a.occ_b[ib]);
       }
       dsh[r] = d;
 #pragma unroll
@@ -696,7 +700,8 @@ struct SampleOut {
 };
 
 // pass 2: write the kept pairs in index order (block offsets from the host scan)
-__global__ void pair_write_kernel(PairArgs k, const double *__restrict__ hii, const uint32_t *__restrict__ occ_a,
+__global__ void pair_write_kernel(PairArgs k, const double *__restrict__ hii, const double *__restrict__ kxa,
+                                  const double *__restrict__ kxb, const uint32_t *__restrict__ occ_a,
                                   const uint32_t *__restrict__ occ_b, uint32_t nb, size_t n, size_t chunk,
                                   const uint8_t *__restrict__ flags, const uint64_t *__restrict__ offsets,
                                   SampleOut o) {
@@ -723,12 +728,12 @@ __global__ void pair_write_kernel(PairArgs k, const double *__restrict__ hii, co
       pair_ab(k, i, A, B);
       pair_keep(k, i, A, B, p);
       float fe, fr;
-      cont_features((double)k.d[i], hii[i], k.e0, k.inv_rnorm, fe, fr);
-      const size_t ia = i / nb;
+      const size_t ia = i / nb, ib = i - ia * nb;
+      cont_features(hii[i] + kxa[ia] + kxb[ib], k.e0, fe, fr);
       o.fe[pos] = fe;
       o.fr[pos] = fr;
       o.oa[pos] = occ_a[ia];
-      o.ob[pos] = occ_b[i - ia * nb];
+      o.ob[pos] = occ_b[ib];
       o.a[pos] = (float)A;
       o.b[pos] = (float)B;
       o.w[pos] = (float)(1.0 / p);
@@ -947,19 +952,42 @@ int grow_set(sbd_tpb_precond::Set &s, size_t need, cudaStream_t st) {
   return SBD_TPB_OK;
 }
 
+// pair index of the 8-fold packed integral store: (ij) = max(i,j)(max(i,j)+1)/2 + min(i,j)
+inline size_t pair_of(size_t i, size_t j) { return i > j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
+// Per string: the occupation window around the Fermi level and the sum of the exchange integrals
+// (pq|qp) over its occupied pairs (what separates H_ii from the spin-free diagonal).
 int ensure_occ_windows(sbd_tpb_handle *h) {
   if (h->d_occw_a) return SBD_TPB_OK;
+  const int L = h->L;
   auto win = [](const std::vector<uint64_t> &v) {
     std::vector<uint32_t> o(v.size());
     const int nel = v.empty() ? 0 : __builtin_popcountll(v[0]);
     for (size_t i = 0; i < v.size(); i++) o[i] = occ_window(v[i], nel);
     return o;
   };
+  auto exch = [&](const std::vector<uint64_t> &v) {
+    std::vector<double> o(v.size(), 0.0);
+    for (size_t i = 0; i < v.size(); i++)
+      for (int p = 0; p < L; p++)
+        if ((v[i] >> p) & 1)
+          for (int q = p + 1; q < L; q++)
+            if ((v[i] >> q) & 1) {
+              const size_t pq = pair_of(p, q);
+              o[i] += h->eri_packed[pair_of(pq, pq)];
+            }
+    return o;
+  };
   const std::vector<uint32_t> a = win(h->astr), b = win(h->bstr);
+  const std::vector<double> ka = exch(h->astr), kb = exch(h->bstr);
   TPB_CUDA(cudaMalloc(&h->d_occw_a, sizeof(uint32_t) * std::max<size_t>(1, a.size())));
   TPB_CUDA(cudaMalloc(&h->d_occw_b, sizeof(uint32_t) * std::max<size_t>(1, b.size())));
+  TPB_CUDA(cudaMalloc(&h->d_kx_a, sizeof(double) * std::max<size_t>(1, ka.size())));
+  TPB_CUDA(cudaMalloc(&h->d_kx_b, sizeof(double) * std::max<size_t>(1, kb.size())));
   TPB_CUDA(cudaMemcpy(h->d_occw_a, a.data(), sizeof(uint32_t) * a.size(), cudaMemcpyHostToDevice));
   TPB_CUDA(cudaMemcpy(h->d_occw_b, b.data(), sizeof(uint32_t) * b.size(), cudaMemcpyHostToDevice));
+  TPB_CUDA(cudaMemcpy(h->d_kx_a, ka.data(), sizeof(double) * ka.size(), cudaMemcpyHostToDevice));
+  TPB_CUDA(cudaMemcpy(h->d_kx_b, kb.data(), sizeof(double) * kb.size(), cudaMemcpyHostToDevice));
   return SBD_TPB_OK;
 }
 
@@ -1053,8 +1081,8 @@ int add_step_pairs(sbd_tpb_precond *p, sbd_tpb_handle *h, const DavRecord &rec, 
       break;
     }
     SampleOut o{s.fe, s.fr, s.a, s.b, s.w, s.oa, s.ob};
-    pair_write_kernel<<<nblk, 256, 0, h->stream>>>(a, h->d_hii, h->d_occw_a, h->d_occw_b, (uint32_t)h->bstr.size(),
-                                                   n, chunk, flags, offs, o);
+    pair_write_kernel<<<nblk, 256, 0, h->stream>>>(a, h->d_hii, h->d_kx_a, h->d_kx_b, h->d_occw_a, h->d_occw_b,
+                                                   (uint32_t)h->bstr.size(), n, chunk, flags, offs, o);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
       rc = fail(SBD_TPB_ERR_CUDA, "precond collect: write");
       break;
@@ -1099,6 +1127,8 @@ int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double
   TPB_CHECK(ensure_occ_windows(h));
   InferArgs a{};
   a.hii = h->d_hii;
+  a.kxa = h->d_kx_a;
+  a.kxb = h->d_kx_b;
   a.e0 = e0;
   a.inv_rnorm = rnorm > 0.0 ? 1.0 / rnorm : 0.0;
   a.occ_a = h->d_occw_a;

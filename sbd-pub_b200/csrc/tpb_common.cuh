@@ -170,6 +170,7 @@ struct sbd_tpb_handle {
   // occupation windows of the strings it reads
   struct sbd_tpb_precond *precond = nullptr;
   uint32_t *d_occw_a = nullptr, *d_occw_b = nullptr;
+  double *d_kx_a = nullptr, *d_kx_b = nullptr;  // same-spin exchange sum of each string
   uint32_t *d_mlp_idx = nullptr;  // determinants selected for the learned correction (+ counter)
   size_t ndet() const { return astr.size() * bstr.size(); }
 };

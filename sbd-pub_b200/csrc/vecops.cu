@@ -247,40 +247,51 @@ __global__ void axpby_kernel(const T *__restrict__ x, T *__restrict__ y, double 
 }
 
 // t <- (t + t^T) / 2 for a square nb x nb vector (alpha and beta strings identical), in place,
-// one 32 x 32 tile pair (bi <= bj) at a time; partials[block] = sum of the new t^2 over the
-// block's tile pairs (fixed assignment, so the sum is deterministic).
+// one 64 x 64 tile pair (bi <= bj) at a time through shared memory (16 independent loads per
+// thread and tile); partials[block] = sum of the new t^2 over the block's tile pairs (fixed
+// assignment, so the sum is deterministic).
+constexpr int kSymTile = 64;
+
 template <typename T>
 __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint32_t nb, double *partials) {
-  __shared__ T A[32][33], B[32][33];
-  const uint32_t T_ = (nb + 31) / 32;
-  const size_t npairs = (size_t)T_ * T_;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  extern __shared__ __align__(16) unsigned char sym_smem[];
+  T(*A)[kSymTile + 1] = reinterpret_cast<T(*)[kSymTile + 1]>(sym_smem);
+  T(*B)[kSymTile + 1] = A + kSymTile;
+  const uint32_t nt = (nb + kSymTile - 1) / kSymTile;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int tx = threadIdx.x & (kSymTile - 1), ty = threadIdx.x / kSymTile;  // 64 x 4
+  constexpr int kRowStep = 256 / kSymTile;
   double acc = 0.0;
   for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
-    const uint32_t bi = (uint32_t)(p / T_), bj = (uint32_t)(p % T_);
-    if (bi > bj) continue;
+    // p -> (bi, bj), bi <= bj, row-major over the upper triangle
+    uint32_t bi = (uint32_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
+    while (bi > 0 && (size_t)bi * nt - (size_t)bi * (bi - 1) / 2 > p) bi--;
+    while ((size_t)(bi + 1) * nt - (size_t)(bi + 1) * bi / 2 <= p) bi++;
+    const uint32_t bj = bi + (uint32_t)(p - ((size_t)bi * nt - (size_t)bi * (bi - 1) / 2));
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-      const uint32_t i = bi * 32 + r, j = bj * 32 + tx;
+#pragma unroll
+    for (int r = ty; r < kSymTile; r += kRowStep) {
+      const uint32_t i = bi * kSymTile + r, j = bj * kSymTile + tx;
       A[r][tx] = (i < nb && j < nb) ? t[(size_t)i * nb + j] : T(0);
-      const uint32_t i2 = bj * 32 + r, j2 = bi * 32 + tx;
+      const uint32_t i2 = bj * kSymTile + r, j2 = bi * kSymTile + tx;
       B[r][tx] = (i2 < nb && j2 < nb) ? t[(size_t)i2 * nb + j2] : T(0);
     }
     __syncthreads();
     const double mult = bi == bj ? 1.0 : 2.0;
-    for (int r = ty; r < 32; r += 8) {
+#pragma unroll
+    for (int r = ty; r < kSymTile; r += kRowStep) {
       // new A[r][c] = (A[r][c] + B[c][r]) / 2, written to both (i, j) and (j, i)
-      const uint32_t i = bi * 32 + r, j = bj * 32 + tx;
+      const uint32_t i = bi * kSymTile + r, j = bj * kSymTile + tx;
       const T v = (T)(((double)A[r][tx] + (double)B[tx][r]) * 0.5);
       if (i < nb && j < nb) {
         t[(size_t)i * nb + j] = v;
         acc += mult * (double)v * (double)v;
       }
     }
-    __syncthreads();
     if (bi != bj) {
-      for (int r = ty; r < 32; r += 8) {
-        const uint32_t i2 = bj * 32 + r, j2 = bi * 32 + tx;
+#pragma unroll
+      for (int r = ty; r < kSymTile; r += kRowStep) {
+        const uint32_t i2 = bj * kSymTile + r, j2 = bi * kSymTile + tx;
         const T v = (T)(((double)A[tx][r] + (double)B[r][tx]) * 0.5);
         if (i2 < nb && j2 < nb) t[(size_t)i2 * nb + j2] = v;
       }
@@ -389,7 +400,9 @@ int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
   const uint32_t nb = (uint32_t)h->bstr.size();
   const int nblk = vec_blocks(h);
   TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nblk + kMaxVec + 3));
-  symmetrize_kernel<T><<<nblk, 256, 0, h->stream>>>(t, nb, h->d_partials);
+  const size_t smem = 2 * kSymTile * (kSymTile + 1) * sizeof(T);
+  TPB_CUDA(cudaFuncSetAttribute(symmetrize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  symmetrize_kernel<T><<<nblk, 256, smem, h->stream>>>(t, nb, h->d_partials);
   TPB_LAUNCHED(h);
   return finish_reduce(h, 1, tt);
 }

@@ -5,7 +5,8 @@
 // " Sample-based diagonalization: ..."), same 1pRDM.txt / 2pRDM.txt files and energy
 // decomposition (main.cc:196-319).  Extra flags select the arithmetic and the correction:
 //   --precision fp64|mixed   --preconditioner diagonal|learned   --device N
-// Flags for parts outside this build (--loadname/--savename, carry-over selection,
+// --loadname / --savename read and write the reference's one-rank wavefunction file
+// (tpb/restart.h).  Flags for parts outside this build (carry-over selection,
 // --dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
 #include <chrono>
 #include <cstdio>
@@ -29,7 +30,7 @@ namespace {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string adetfile = "alphadets.txt", bdetfile, fcidumpfile = "fcidump.txt";
+  std::string adetfile = "alphadets.txt", bdetfile, fcidumpfile = "fcidump.txt", loadname, savename;
   sbd_tpb_params prm;
   sbd_tpb_default_params(&prm);
   prm.verbose = 1;
@@ -60,7 +61,9 @@ int main(int argc, char **argv) {
              a == "--carryover_adetfile" || a == "--carryover_bdetfile") next();
     else if (a == "--adet_comm_size" || a == "--bdet_comm_size" || a == "--task_comm_size")
       comm_sizes *= std::atoi(next().c_str());
-    else if (a == "--loadname" || a == "--savename" || a == "--dump_matrix_form_wf") {
+    else if (a == "--loadname") loadname = next();
+    else if (a == "--savename") savename = next();
+    else if (a == "--dump_matrix_form_wf") {
       const std::string v = next();
       if (!v.empty()) unsupported += " " + a;
     } else if (a == "--precision") {
@@ -77,7 +80,7 @@ int main(int argc, char **argv) {
     else if (a == "--use_precalculated_dets" || a == "--max_memory_gb_for_determinants" ||
              a == "--thrust_collapse_loops") next();
   }
-  (void)bit_length;
+  if (bit_length == 0 || bit_length > 64) die("--bit_length must be in [1, 64]");
   if (method != 0) die("only --method 0 (matrix-free Davidson) is built");
   if (comm_sizes != 1) die("one rank on one GPU: --*_comm_size must be 1");
   if (prm.init != 0) die("only --init 0 (start from the first determinant) is built");
@@ -111,8 +114,21 @@ int main(int argc, char **argv) {
   res.density = density.data();
   res.one_rdm = prm.do_rdm ? one.data() : nullptr;
   res.two_rdm = prm.do_rdm ? two.data() : nullptr;
-  const int rc = sbd_tpb_diag(&prm, &ham, adet.data(), na, bdet.data(), nb, &res);
+  // initial vector: HF determinant, or a stored wavefunction (tpb/sbdiag.h:280-296)
+  std::vector<double> W0;
+  if (!loadname.empty()) {
+    const auto t0 = std::chrono::steady_clock::now();
+    size_t matched = 0;
+    if (!tpbio::load_wavefunction(loadname, L, bit_length, adet, bdet, W0, &matched, &err)) die(err);
+    if (matched == 0) die("no stored amplitude matches the current strings: " + loadname);
+    std::cout << " Elapsed time for init "
+              << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << " (sec) "
+              << std::endl;
+  }
+  const int rc = sbd_tpb_diag_from(&prm, &ham, adet.data(), na, bdet.data(), nb, W0.empty() ? nullptr : W0.data(),
+                                   &res);
   if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(sbd_tpb_last_error());
+  if (!savename.empty() && !tpbio::save_wavefunction(savename, L, bit_length, adet, bdet, W, &err)) die(err);
   std::cout << " Elapsed time for helper construction " << res.seconds_tables << " (sec) " << std::endl;
   std::cout << " Elapsed time for davidson " << res.seconds_davidson << " (sec) " << std::endl;
   std::cout << " Energy = " << res.energy << std::endl;

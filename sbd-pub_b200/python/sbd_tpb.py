@@ -34,7 +34,7 @@ PRECOND_DIAGONAL, PRECOND_LEARNED = 0, 1
 
 # Every function the header declares (the symbol test checks the library against this list).
 EXPORTED = [
-    "sbd_tpb_default_params", "sbd_tpb_diag", "sbd_tpb_last_error", "sbd_tpb_create",
+    "sbd_tpb_default_params", "sbd_tpb_diag", "sbd_tpb_diag_from", "sbd_tpb_last_error", "sbd_tpb_create",
     "sbd_tpb_destroy", "sbd_tpb_set_hamiltonian", "sbd_tpb_set_strings", "sbd_tpb_build_tables",
     "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
     "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_sigma_noalloc", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
@@ -96,6 +96,8 @@ def lib():
     L.sbd_tpb_default_params.argtypes = [C.POINTER(Params)]
     L.sbd_tpb_diag.argtypes = [C.POINTER(Params), C.POINTER(Hamiltonian), vp, C.c_size_t, vp,
                                C.c_size_t, C.POINTER(Result)]
+    L.sbd_tpb_diag_from.argtypes = [C.POINTER(Params), C.POINTER(Hamiltonian), vp, C.c_size_t, vp,
+                                    C.c_size_t, vp, C.POINTER(Result)]
     L.sbd_tpb_create.argtypes = [C.c_int, C.POINTER(vp)]
     L.sbd_tpb_destroy.argtypes = [vp]
     L.sbd_tpb_set_hamiltonian.argtypes = [vp, C.POINTER(Hamiltonian)]

@@ -2,7 +2,8 @@
 library's BF16 training kernels and fused inference kernel against the oracle, training on pairs
 collected from plain Davidson runs, and the learned solve's answer against the FP64 one (GPU).
 
-The network: x (64) -> 256 -> GELU -> 256 -> GELU -> y, correction t = d (1 + y).
+The network: x (64) -> 256 -> GELU -> 256 -> GELU -> y, correction t = d (1 + y); x depends only on
+a determinant's spatial occupation, so y is the same across a spin-coupled set.
 """
 import numpy as np
 import pytest
@@ -30,18 +31,31 @@ def occ_window(s, nel):
     return bits
 
 
-def features(d, hd, e0, rnorm, wa, wb):
-    """Feature rows as the inference kernel forms them (before BF16 rounding)."""
-    den = e0 - hd
-    den = np.where(np.abs(den) > 1e-12, den, den - 1e-12)
-    r = d * den
-    fe = np.arcsinh((hd - e0).astype(np.float32)) * np.float32(0.25)
-    fr = np.arcsinh((r / rnorm * 1e4).astype(np.float32)) * np.float32(0.1)
-    x = np.zeros((len(d), F), np.float32)
-    x[:, 0], x[:, 1] = fe, fr
-    x[:, 2:2 + WIN] = wa
-    x[:, 2 + WIN:2 + 2 * WIN] = wb
+def features(hdJ, e0, wa, wb):
+    """Feature rows as the inference kernel forms them (before BF16 rounding): the spin-free
+    diagonal, a zero residual slot, doubly and singly occupied windows."""
+    x = np.zeros((len(hdJ), F), np.float32)
+    x[:, 0] = np.arcsinh((hdJ - e0).astype(np.float32)) * np.float32(0.25)
+    x[:, 2:2 + WIN] = wa * wb
+    x[:, 2 + WIN:2 + 2 * WIN] = (wa + wb) % 2
     return x
+
+
+def pair_of(i, j):
+    return i * (i + 1) // 2 + j if i > j else j * (j + 1) // 2 + i
+
+
+def exchange_sums(prob, strs):
+    """Sum of (pq|qp) over the occupied pairs of each string."""
+    L = prob.norb
+    out = np.zeros(len(strs))
+    for n, s in enumerate(strs):
+        occ = [p for p in range(L) if (int(s) >> p) & 1]
+        for a_ in range(len(occ)):
+            for b_ in range(a_ + 1, len(occ)):
+                pq = pair_of(occ[a_], occ[b_])
+                out[n] += prob.eri_packed[pair_of(pq, pq)]
+    return out
 
 
 def np_forward64(x, W1, b1, W2, b2, w3, b3):
@@ -161,7 +175,8 @@ def test_gpu_mlp_inference_kernel_vs_oracle():
     nel_b = bin(int(prob.bstr[0])).count("1")
     wa = np.array([occ_window(s, nel_a) for s in prob.astr])
     wb = np.array([occ_window(s, nel_b) for s in prob.bstr])
-    x = features(d, hd, e0, rnorm, np.repeat(wa, nb, axis=0), np.tile(wb, (na, 1)))
+    hdJ = hd + np.repeat(exchange_sums(prob, prob.astr), nb) + np.tile(exchange_sums(prob, prob.bstr), na)
+    x = features(hdJ, e0, np.repeat(wa, nb, axis=0), np.tile(wb, (na, 1)))
     Pb = [bf16(P[0]), P[1], bf16(P[2]), P[3], P[4], P[5]]
     y_ref = pyoracle.mlp_forward(bf16(x), *Pb).astype(np.float64)
     y_gpu = t / np.where(d != 0, d, 1.0) - 1.0
@@ -202,7 +217,9 @@ def test_gpu_mlp_inference_budgeted_subset():
     nel = bin(int(prob.astr[0])).count("1")
     wa = np.array([occ_window(prob.astr[i // nb], nel) for i in sel])
     wb = np.array([occ_window(prob.bstr[i % nb], nel) for i in sel])
-    x = features(d[sel], hd[sel], e0, rnorm, wa, wb)
+    kxa = exchange_sums(prob, prob.astr[sel // nb])
+    kxb = exchange_sums(prob, prob.bstr[sel % nb])
+    x = features(hd[sel] + kxa + kxb, e0, wa, wb)
     one = np.ones(len(sel), np.float32)
     _, _, y_train = pc.gradients(bf16(x), one, one, one)
     y_gpu = t[sel] / d[sel] - 1.0
