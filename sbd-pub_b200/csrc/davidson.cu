@@ -12,10 +12,14 @@
 // double.  The mixed path stores C/HC/W/t in FP32, computes sigma of (H - s) with s = H_00 so the
 // FP32 entries carry residual-sized values, keeps all dot products and the Rayleigh-Ritz in FP64,
 // and finishes with one FP64 sigma on the converged vector for the reported energy and residual.
-// Both orthogonalise with classical Gram-Schmidt, repeated once when the first round cancels more
-// than half of |t|^2 (as stable as the reference's modified Gram-Schmidt, tpb/davidson.h:871-879,
-// with one or two fused passes instead of k+1).  The converged vector stays in HBM for the final
-// sigma and the RDMs; it crosses to the host only when the caller asks for it.
+// With a learned preconditioner attached, the first four restart cycles alternate between the
+// diagonal and the learned correction and later cycles use the learned one only if its cycles
+// lowered the residual more than 10% faster per step; inside a learned cycle a step whose residual
+// did not drop is followed by a diagonal step.  Both precisions orthogonalise with classical Gram-Schmidt, repeated once
+// when the first round cancels more than half of |t|^2 (as stable as the reference's modified
+// Gram-Schmidt, tpb/davidson.h:871-879, with one or two fused passes instead of k+1).  The
+// converged vector stays in HBM for the final sigma and the RDMs; it crosses to the host only when
+// the caller asks for it.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -149,6 +153,12 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
   double energy = 0.0, prev_norm = 0.0;
   bool prev_learned = false;
   int nlearned = 0, nfallback = 0;
+  // Which correction a cycle uses: the first four cycles alternate learned / diagonal, then every
+  // cycle uses the one whose cycles lowered log|r| faster per step (ties: diagonal).
+  double rate_sum[2] = {0.0, 0.0};  // [0] diagonal, [1] learned
+  int rate_cnt[2] = {0, 0};
+  int cycle_mode = 0, cycle_steps = 0;
+  double cycle_r0 = 0.0;
   std::vector<int> rec_cycle;  // basis indices of the current cycle (recording)
   const auto t_start = std::chrono::steady_clock::now();
 
@@ -159,6 +169,18 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       f[0] = 1.0 / std::sqrt(ww);
       w_current = false;
     }
+    if (learned) {
+      if (it < 4) {
+        // diagonal first: convergence slows as it proceeds, so the learned cycles (later in each
+        // pair) are measured at a disadvantage and must really be faster to be kept
+        cycle_mode = (it % 2 == 0) ? 0 : 1;
+      } else {
+        const double rl = rate_cnt[1] ? rate_sum[1] / rate_cnt[1] : 0.0;
+        const double rd = rate_cnt[0] ? rate_sum[0] / rate_cnt[0] : 0.0;
+        cycle_mode = rl > 1.1 * rd ? 1 : 0;
+      }
+    }
+    cycle_steps = 0;
     for (int ib = 0; ib < nb; ib++) {
       const auto s0 = std::chrono::steady_clock::now();
       TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
@@ -218,16 +240,18 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       }
       // learned correction: used unless the previous step was a learned one that did not lower
       // the residual, in which case this step falls back to the diagonal correction
+      if (ib == 0) cycle_r0 = norm_R;
+      cycle_steps++;
+      if (learned && (last || norm_R < prm->eps) && cycle_steps > 1 && cycle_r0 > 0.0 && norm_R > 0.0) {
+        // the cycle's rate of residual reduction, for the choice of the next cycles' correction
+        rate_sum[cycle_mode] += std::log(cycle_r0 / norm_R) / (cycle_steps - 1);
+        rate_cnt[cycle_mode]++;
+      }
       bool use_learned = false;
-      if (learned && !last) {
+      if (learned && cycle_mode == 1 && !last) {
         const bool failed = ib > 0 && prev_learned && !(norm_R < prev_norm);
         use_learned = !failed;
         if (failed) nfallback++;
-        // a network that keeps failing on this problem is switched off for the rest of the solve
-        if (nlearned >= 8 && 3 * nfallback > nlearned) {
-          learned = nullptr;
-          use_learned = false;
-        }
       }
       prev_learned = use_learned;
       prev_norm = norm_R;

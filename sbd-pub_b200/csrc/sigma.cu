@@ -345,9 +345,10 @@ __global__ void __launch_bounds__(256)
       }
       __syncthreads();
     }
-    for (uint32_t q = threadIdx.x; q < a.ncols_s; q += blockDim.x) {
+    // sum over the beta singles of compact column q (its column index in ib)
+    auto column = [&](uint32_t q, uint32_t &ib) -> double {
       const uint2 c0 = __ldg(&a.colp[q]), c1 = __ldg(&a.colp[q + 1]);
-      const uint32_t ib = c0.x;
+      ib = c0.x;
       double acc = 0.0;
       for (uint32_t f = c0.y; f < c1.y; f++) {
         const uint2 be = __ldg(&a.bsp[f]);
@@ -366,7 +367,21 @@ __global__ void __launch_bounds__(256)
         }
         acc += pb > 0 ? sum : -sum;
       }
-      srow[ib] = (T)((double)srow[ib] + acc);
+      return acc;
+    };
+    // two independent columns per iteration, so their load chains overlap
+    uint32_t q = threadIdx.x;
+    for (; q + blockDim.x < a.ncols_s; q += 2 * blockDim.x) {
+      uint32_t ib0, ib1;
+      const double s0 = column(q, ib0), s1 = column(q + blockDim.x, ib1);
+      const T o0 = srow[ib0], o1 = srow[ib1];
+      srow[ib0] = (T)((double)o0 + s0);
+      srow[ib1] = (T)((double)o1 + s1);
+    }
+    if (q < a.ncols_s) {
+      uint32_t ib0;
+      const double s0 = column(q, ib0);
+      srow[ib0] = (T)((double)srow[ib0] + s0);
     }
   }
 }
