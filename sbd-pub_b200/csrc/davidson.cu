@@ -90,9 +90,19 @@ void jacobi_eigen(int n, const double *A, int lda, std::vector<double> &E, std::
 
 template <typename T>
 struct DevVec {
+  sbd_tpb_handle *h = nullptr;
   T *p = nullptr;
+  size_t bytes = 0;
+  int get(sbd_tpb_handle *hh, size_t count) {
+    h = hh;
+    bytes = count * sizeof(T);
+    void *q = nullptr;
+    const int rc = pool_get(h, bytes, &q);
+    p = static_cast<T *>(q);
+    return rc;
+  }
   ~DevVec() {
-    if (p) cudaFree(p);
+    if (p) pool_put(h, p, bytes);
   }
 };
 
@@ -106,10 +116,10 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
   std::vector<DevVec<T>> S(nb), HS(nb);
   DevVec<T> Wv;
   for (int k = 0; k < nb; k++) {
-    TPB_CUDA(cudaMalloc(&S[k].p, sizeof(T) * n));
-    TPB_CUDA(cudaMalloc(&HS[k].p, sizeof(T) * n));
+    TPB_CHECK(S[k].get(h, n));
+    TPB_CHECK(HS[k].get(h, n));
   }
-  TPB_CUDA(cudaMalloc(&Wv.p, sizeof(T) * n));
+  TPB_CHECK(Wv.get(h, n));
 
   // Subspace vectors are stored unnormalised: the basis vector is C_k = f_k S_k and
   // H C_k = f_k sigma(S_k), so normalising costs no pass over the vector.
@@ -210,7 +220,27 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       ra.W = last ? Wv.p : nullptr;
       T *tnext = last ? nullptr : S[ib + 1].p;
       ra.t = tnext;
-      TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+      // Fast path: residual, symmetric projection and the first Gram-Schmidt round go back to back
+      // (the CGS kernel reads the overlaps from device memory) and their scalars come back with
+      // one synchronisation.  If this step turns out converged, the extra work on t is discarded.
+      const bool fast = !rec && !last && !(learned && cycle_mode == 1);
+      double t0_fast = 0.0, tt_fast = 0.0;
+      if (fast) {
+        constexpr int kSymSlot = 20, kCgsSlot = 24;
+        TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
+        if (sym) TPB_CHECK(symmetrize_async<T>(h, tnext, kSymSlot));
+        std::vector<double> coef(ib + 1);
+        for (int k = 0; k <= ib; k++) coef[k] = f[k] * f[k];
+        TPB_CHECK(cgs_update_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, n, 1, kCgsSlot));
+        const double *sc = fetch_scalars(h, kCgsSlot + ib + 2);
+        if (!sc) return SBD_TPB_ERR_CUDA;
+        for (int k = 0; k < ib + 4; k++) out[k] = sc[k];
+        t0_fast = sym ? sc[kSymSlot] : sc[2 + ib + 1];
+        tt_fast = sc[kCgsSlot];
+        for (int k = 0; k <= ib; k++) dots[1 + k] = sc[kCgsSlot + 1 + k];
+      } else {
+        TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+      }
       w_current = last;
       m_last = ib + 1;
       ww = out[0];
@@ -268,7 +298,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       }
       if (use_learned)
         TPB_CHECK(precond_apply<T>(h, learned, tnext, ra.e0, std::sqrt(out[1]), out[2 + ib + 1]));
-      if (sym && !last) {
+      if (sym && !last && !fast) {
         // the S_k are exactly symmetric, so S_k.t is unchanged by the projection; only t.t is
         TPB_CHECK(symmetrize<T>(h, tnext, &out[2 + ib + 1]));
       }
@@ -286,11 +316,14 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         // A second round runs only when the first cancelled more than half of |t|^2 ("twice is
         // enough": after a round that keeps |t|^2 >= 1/2 of its input, t is orthogonal to the
         // subspace to working precision).
-        const double t0 = out[2 + ib + 1];
+        double t0 = t0_fast, tt = tt_fast;
         std::vector<double> o(ib + 1);
-        for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * out[2 + k];
-        TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 1, dots.data()));
-        double tt = dots[0];
+        if (!fast) {
+          t0 = out[2 + ib + 1];
+          for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * out[2 + k];
+          TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 1, dots.data()));
+          tt = dots[0];
+        }
         if (tt < 0.5 * t0) {
           for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * dots[1 + k];
           TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 0, dots.data()));
@@ -377,7 +410,7 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   }
   int nl = 0, nf = 0;
   DevVec<double> dW, dHW;
-  TPB_CUDA(cudaMalloc(&dW.p, sizeof(double) * n));
+  TPB_CHECK(dW.get(h, n));
   if (p->precision == SBD_TPB_MIXED) {
     double h00 = 0.0;
     TPB_CUDA(cudaMemcpy(&h00, h->d_hii, sizeof(double), cudaMemcpyDeviceToHost));
@@ -388,7 +421,7 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   res->learned_steps = nl;
   res->fallback_steps = nf;
   // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
-  TPB_CUDA(cudaMalloc(&dHW.p, sizeof(double) * n));
+  TPB_CHECK(dHW.get(h, n));
   double E = 0.0, rr = 0.0;
   TPB_CHECK(sigma_sep<double>(h, dW.p, dHW.p, 0));
   const double *wp[1] = {dW.p};
@@ -402,14 +435,44 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
                              h->stream));
   }
   TPB_CUDA(cudaStreamSynchronize(h->stream));
-  if (res->density || res->one_rdm || res->two_rdm)
+  if (res->density || res->one_rdm || res->two_rdm) {
+    if (res->one_rdm || res->two_rdm) pool_clear(h);  // the 2-RDM passes need their own N-vectors
     TPB_CHECK(rdm_sep(h, dW.p, res->one_rdm, res->two_rdm, res->density));
+  }
   res->energy = E;
   res->residual = (p->precision == SBD_TPB_MIXED) ? std::sqrt(rr) : resid;
   res->iterations = nsig;
   res->converged = conv;
   res->seconds_davidson = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return conv ? SBD_TPB_OK : SBD_TPB_ERR_NOT_CONVERGED;
+}
+
+int pool_get(sbd_tpb_handle *h, size_t bytes, void **out) {
+  *out = nullptr;
+  size_t best = h->vec_pool.size();
+  for (size_t i = 0; i < h->vec_pool.size(); i++) {
+    const size_t b = h->vec_pool[i].second;
+    if (b >= bytes && b <= 2 * bytes && (best == h->vec_pool.size() || b < h->vec_pool[best].second)) best = i;
+  }
+  if (best < h->vec_pool.size()) {
+    *out = h->vec_pool[best].first;
+    h->vec_pool.erase(h->vec_pool.begin() + best);
+    return SBD_TPB_OK;
+  }
+  if (cudaMalloc(out, bytes) == cudaSuccess) return SBD_TPB_OK;
+  cudaGetLastError();
+  pool_clear(h);
+  TPB_CUDA(cudaMalloc(out, bytes));
+  return SBD_TPB_OK;
+}
+
+void pool_put(sbd_tpb_handle *h, void *p, size_t bytes) {
+  if (p) h->vec_pool.emplace_back(p, bytes);
+}
+
+void pool_clear(sbd_tpb_handle *h) {
+  for (auto &b : h->vec_pool) cudaFree(b.first);
+  h->vec_pool.clear();
 }
 
 int davidson_record(sbd_tpb_handle *h, const sbd_tpb_params *p, DavRecord *rec, double *Psi,

@@ -179,8 +179,12 @@ void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->ab.Vlo);
   free_dev(h->ab.err);
   h->ab = ABDense();
+  pool_clear(h);
   free_dev(h->d_partials);
   h->partials_cap = 0;
+  free_dev(h->d_scal);
+  if (h->h_scal) cudaFreeHost(h->h_scal);
+  h->h_scal = nullptr;
   free_dev(h->d_tmp64);
   free_dev(h->d_tmp64b);
   free_dev(h->d_tmp32);

@@ -152,6 +152,10 @@ struct sbd_tpb_handle {
   // scratch
   double *d_partials = nullptr;  // reduction partial sums
   size_t partials_cap = 0;
+  double *d_scal = nullptr, *h_scal = nullptr;  // reduction results read back together (pinned)
+  // N-vectors of finished Davidson runs kept for the next run (allocating tens of GB per solve
+  // costs a noticeable and variable fraction of a solve); freed with the problem
+  std::vector<std::pair<void *, size_t>> vec_pool;
   double *d_tmp64 = nullptr;     // one N-vector FP64 (sign conversion staging)
   double *d_tmp64b = nullptr;
   float *d_tmp32 = nullptr, *d_tmp32b = nullptr;
@@ -209,6 +213,12 @@ int multi_dot(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n,
 // rdm.cu
 // W: device FP64 vector in the separated convention; outputs are host arrays (any may be null):
 // one [2L^2], two [4L^4] in the reference layouts, density [2L].
+// vector pool (davidson.cu): a block of at least `bytes` (reused if one of at most twice the size
+// is free, else cudaMalloc, emptying the pool and retrying once if memory is short), its return,
+// and the release of every kept block
+int pool_get(sbd_tpb_handle *h, size_t bytes, void **out);
+void pool_put(sbd_tpb_handle *h, void *p, size_t bytes);
+void pool_clear(sbd_tpb_handle *h);
 int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double *density);
 // davidson.cu
 int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,

@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kVecThreads) residual_kernel(ResidualArgs<T> a
 template <typename T, int M, bool kDots>
 struct CgsBody {
   const VecPtrs<T> &C;
-  const CoefArray &o;
+  const double (&o)[M];
   T *t;
   double (&acc)[M + 1];
   template <int W>
@@ -196,7 +196,7 @@ struct CgsBody {
     for (int k = 0; k < M; k++) {
       ldv<T, W>(C.p[k] + i, c[k]);
 #pragma unroll
-      for (int l = 0; l < W; l++) x[l] -= o.v[k] * (double)c[k][l];
+      for (int l = 0; l < W; l++) x[l] -= o[k] * (double)c[k][l];
     }
     T xt[W];
 #pragma unroll
@@ -212,12 +212,17 @@ struct CgsBody {
   }
 };
 
+// o_k = co.v[k] * (ov ? ov[k] : 1): the overlaps may come straight from a device reduction
 template <typename T, int M, bool kDots>
 __global__ void __launch_bounds__(kVecThreads)
-    cgs_update_kernel(VecPtrs<T> C, CoefArray o, T *__restrict__ t, size_t n, double *partials) {
+    cgs_update_kernel(VecPtrs<T> C, CoefArray co, const double *__restrict__ ov, T *__restrict__ t, size_t n,
+                      double *partials) {
   double acc[M + 1];
 #pragma unroll
   for (int j = 0; j < M + 1; j++) acc[j] = 0.0;
+  double o[M];
+#pragma unroll
+  for (int k = 0; k < M; k++) o[k] = co.v[k] * (ov ? __ldg(&ov[k]) : 1.0);
   CgsBody<T, M, kDots> b{C, o, t, acc};
   for_each_group<T>(n, b);
   block_reduce_store<M + 1>(acc, kDots ? M + 1 : 1, partials, gridDim.x);
@@ -315,6 +320,21 @@ int ensure_partials(sbd_tpb_handle *h, size_t n) {
 
 int vec_blocks(sbd_tpb_handle *h) { return h->num_sms * 4; }
 
+// device slots for reductions whose results are read back together (pinned host mirror)
+static int ensure_scalars(sbd_tpb_handle *h) {
+  if (h->d_scal) return SBD_TPB_OK;
+  TPB_CUDA(cudaMalloc(&h->d_scal, sizeof(double) * kScalarSlots));
+  TPB_CUDA(cudaMallocHost(&h->h_scal, sizeof(double) * kScalarSlots));
+  return SBD_TPB_OK;
+}
+
+static int reduce_into(sbd_tpb_handle *h, int nvals, double *d_dst) {
+  const int nb = vec_blocks(h);
+  reduce_partials_kernel<<<nvals, 256, 0, h->stream>>>(h->d_partials, nb, d_dst);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
 static int finish_reduce(sbd_tpb_handle *h, int nvals, double *host_out) {
   const int nb = vec_blocks(h);
   double *d_out = h->d_partials + (size_t)(kMaxVec + 3) * nb;
@@ -372,31 +392,73 @@ int residual_step(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, double 
 }
 
 template <typename T>
-int cgs_update(sbd_tpb_handle *h, const T *const *C, int m, const double *o, T *t, size_t n,
-               int want_dots, double *out) {
+static int launch_cgs(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, const double *ov_dev, T *t,
+                      size_t n, int want_dots) {
   if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
   const int nb = vec_blocks(h);
   TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
   VecPtrs<T> P;
   CoefArray co;
   for (int j = 0; j < kMaxVec; j++) P.p[j] = j < m ? C[j] : nullptr;
-  for (int j = 0; j < kMaxSub; j++) co.v[j] = j < m ? o[j] : 0.0;
-  TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
+  for (int j = 0; j < kMaxSub; j++) co.v[j] = j < m ? coef[j] : 0.0;
+  return dispatch_n<1>(m, [&](auto K) {
     constexpr int M = decltype(K)::value;
     if constexpr (M <= kMaxSub) {
       if (want_dots)
-        cgs_update_kernel<T, M, true><<<nb, kVecThreads, 0, h->stream>>>(P, co, t, n, h->d_partials);
+        cgs_update_kernel<T, M, true><<<nb, kVecThreads, 0, h->stream>>>(P, co, ov_dev, t, n, h->d_partials);
       else
-        cgs_update_kernel<T, M, false><<<nb, kVecThreads, 0, h->stream>>>(P, co, t, n, h->d_partials);
+        cgs_update_kernel<T, M, false><<<nb, kVecThreads, 0, h->stream>>>(P, co, ov_dev, t, n, h->d_partials);
       TPB_LAUNCHED(h);
     }
     return SBD_TPB_OK;
-  }));
+  });
+}
+
+template <typename T>
+int cgs_update(sbd_tpb_handle *h, const T *const *C, int m, const double *o, T *t, size_t n,
+               int want_dots, double *out) {
+  TPB_CHECK(launch_cgs<T>(h, C, m, o, nullptr, t, n, want_dots));
   return finish_reduce(h, want_dots ? 1 + m : 1, out);
 }
 
 template <typename T>
-int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
+int residual_step_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, int slot) {
+  if (a.m < 1 || a.m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  const int nb = vec_blocks(h);
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
+  TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      residual_kernel<T, M><<<nb, kVecThreads, 0, h->stream>>>(a, n, h->d_partials);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, a.m + 3, h->d_scal + slot);
+}
+
+template <typename T>
+int cgs_update_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                     size_t n, int want_dots, int slot) {
+  TPB_CHECK(ensure_scalars(h));
+  TPB_CHECK(launch_cgs<T>(h, C, m, coef, h->d_scal + ov_slot, t, n, want_dots));
+  return reduce_into(h, want_dots ? 1 + m : 1, h->d_scal + slot);
+}
+
+const double *fetch_scalars(sbd_tpb_handle *h, int count) {
+  if (ensure_scalars(h) != SBD_TPB_OK) return nullptr;
+  if (cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    fail(SBD_TPB_ERR_CUDA, "fetching reduction results failed");
+    return nullptr;
+  }
+  return h->h_scal;
+}
+
+template <typename T>
+static int launch_symmetrize(sbd_tpb_handle *h, T *t) {
   const uint32_t nb = (uint32_t)h->bstr.size();
   const int nblk = vec_blocks(h);
   TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nblk + kMaxVec + 3));
@@ -404,6 +466,19 @@ int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
   TPB_CUDA(cudaFuncSetAttribute(symmetrize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   symmetrize_kernel<T><<<nblk, 256, smem, h->stream>>>(t, nb, h->d_partials);
   TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+template <typename T>
+int symmetrize_async(sbd_tpb_handle *h, T *t, int slot) {
+  TPB_CHECK(ensure_scalars(h));
+  TPB_CHECK(launch_symmetrize<T>(h, t));
+  return reduce_into(h, 1, h->d_scal + slot);
+}
+
+template <typename T>
+int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
+  TPB_CHECK(launch_symmetrize<T>(h, t));
   return finish_reduce(h, 1, tt);
 }
 
@@ -439,6 +514,14 @@ template int cgs_update<double>(sbd_tpb_handle *, const double *const *, int, co
                                 double *, size_t, int, double *);
 template int cgs_update<float>(sbd_tpb_handle *, const float *const *, int, const double *,
                                float *, size_t, int, double *);
+template int residual_step_async<double>(sbd_tpb_handle *, const ResidualArgs<double> &, size_t, int);
+template int residual_step_async<float>(sbd_tpb_handle *, const ResidualArgs<float> &, size_t, int);
+template int cgs_update_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, int, double *,
+                                      size_t, int, int);
+template int cgs_update_async<float>(sbd_tpb_handle *, const float *const *, int, const double *, int, float *,
+                                     size_t, int, int);
+template int symmetrize_async<double>(sbd_tpb_handle *, double *, int);
+template int symmetrize_async<float>(sbd_tpb_handle *, float *, int);
 template int symmetrize<double>(sbd_tpb_handle *, double *, double *);
 template int symmetrize<float>(sbd_tpb_handle *, float *, double *);
 template int scale_vec<double>(sbd_tpb_handle *, double *, double, size_t);

@@ -42,6 +42,19 @@ int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n);
 // t <- (t + t^T)/2 over the square (alpha = beta strings) determinant matrix; tt = new t.t
 template <typename T>
 int symmetrize(sbd_tpb_handle *h, T *t, double *tt);
+
+// The same passes without a host round trip: each reduces into slots of a small device array
+// (kScalarSlots doubles), read back together by fetch_scalars (one stream synchronisation).
+// cgs_update_async takes the overlaps from device slots ov_slot.. (o_k = coef[k] * overlap_k).
+constexpr int kScalarSlots = 64;
+template <typename T>
+int residual_step_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, size_t n, int slot);
+template <typename T>
+int symmetrize_async(sbd_tpb_handle *h, T *t, int slot);
+template <typename T>
+int cgs_update_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                     size_t n, int want_dots, int slot);
+const double *fetch_scalars(sbd_tpb_handle *h, int count);
 template <typename S, typename D>
 int convert_vec(sbd_tpb_handle *h, const S *x, D *y, size_t n);
 template <typename T>
