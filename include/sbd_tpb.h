@@ -207,7 +207,7 @@ SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);
 /* ---- learned Davidson preconditioner ------------------------------------------------------
  * No counterpart in the reference, whose only correction is the diagonal one
  * t = r / (E0 - H_ii) (tpb/davidson.h:858-868).  A small MLP predicts a per-determinant factor:
- *   t_i = d_i * (1 + y_i),  d_i = r_i / (E0 - H_ii),
+ *   t_i = d_i * (1 + 0.5 tanh(y_i)),  d_i = r_i / (E0 - H_ii),
  *   y = w3 . gelu(W2 gelu(W1 x + b1) + b2) + b3   (hidden width 256, tanh-form GELU, BF16
  *   weights and activations on tensor cores, FP32 accumulation),
  * with x = [asinh(E_J - E0)/4, 0, which of the 24 orbitals n-12 .. n+11 around the Fermi level
@@ -235,7 +235,7 @@ SBD_TPB_API int sbd_tpb_precond_collect(sbd_tpb_precond *p, sbd_tpb_handle *h, c
                                         size_t samples_per_step, int role, double *energy);
 SBD_TPB_API int sbd_tpb_precond_num_samples(sbd_tpb_precond *p, int role, size_t *n);
 /* Adam on the training set, minibatches of `batch` (multiple of 128); loss is the weighted mean
- * of (a (1 + y) - b)^2 / 2 with a = d/|d| and b the scaled exact correction. */
+ * of (a (1 + 0.5 tanh(y)) - b)^2 / 2 with a = d/|d| and b the scaled exact correction. */
 SBD_TPB_API int sbd_tpb_precond_train(sbd_tpb_precond *p, int epochs, int batch, double lr, double *last_loss);
 /* Weighted squared error of the learned correction and of the diagonal one (y = 0) on a set. */
 SBD_TPB_API int sbd_tpb_precond_evaluate(sbd_tpb_precond *p, int role, double *loss_learned,
@@ -243,12 +243,12 @@ SBD_TPB_API int sbd_tpb_precond_evaluate(sbd_tpb_precond *p, int role, double *l
 SBD_TPB_API int sbd_tpb_precond_get_params(sbd_tpb_precond *p, float *params, size_t n);
 SBD_TPB_API int sbd_tpb_precond_set_params(sbd_tpb_precond *p, const float *params, size_t n);
 /* One forward/backward pass of the training kernels on n host samples (x: n x 64 features,
- * a, b, w per sample): grad (SBD_TPB_MLP_PARAMS floats) of 0.5/n sum w (a (1 + y) - b)^2, its
- * loss and the outputs y.  For gradient checks. */
+ * a, b, w per sample): grad (SBD_TPB_MLP_PARAMS floats) of 0.5/n sum w (a (1 + 0.5 tanh(y)) - b)^2,
+ * its loss and the bounded outputs 0.5 tanh(y).  For gradient checks. */
 SBD_TPB_API int sbd_tpb_precond_gradients(sbd_tpb_precond *p, size_t n, const float *x, const float *a,
                                           const float *b, const float *w, float *grad, double *loss,
                                           float *y);
-/* The fused inference kernel on the handle's determinants: t = d (1 + y) from d (host, FP64,
+/* The fused inference kernel on the handle's determinants: t = d (1 + 0.5 tanh(y)) from d (host, FP64,
  * separated convention, [na*nb]), E0 and |r|.  Beyond 2^22 determinants only the entries with
  * |d_i| >= |d| / 2^11 are corrected (at most 2^22 of them), as inside the Davidson loop; the
  * others keep t_i = d_i.  For parity tests. */

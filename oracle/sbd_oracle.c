@@ -877,9 +877,11 @@ double orc_mlp_backward(int n, int din, int dh, const float *x, const float *a, 
   double *d2 = malloc((size_t)dh * sizeof(double)), *d1 = malloc((size_t)dh * sizeof(double));
   double loss = 0.0;
   for (int r = 0; r < n; r++) {
-    const double e = (double)a[r] * (1.0 + (double)y[r]) - (double)b[r];
+    /* bounded factor 1 + c tanh(y) of the learned correction */
+    const double th = tanh((double)y[r]);
+    const double e = (double)a[r] * (1.0 + ORC_MLP_BOUND * th) - (double)b[r];
     loss += 0.5 * w[r] * e * e / n;
-    double dy = (double)w[r] * a[r] * e / n;
+    double dy = (double)w[r] * a[r] * e / n * ORC_MLP_BOUND * (1.0 - th * th);
     const float *a1 = h1 + (size_t)r * dh, *a2 = h2 + (size_t)r * dh;
     gb3[0] += dy;
     for (int i = 0; i < dh; i++) {

@@ -120,8 +120,10 @@ void orc_mlp_forward(int n, int din, int dh, const float *x, const float *W1, co
                      const float *W2, const float *b2, const float *W3, const float *b3,
                      float *h1_out, float *h2_out, float *y);
 /* Gradients, with respect to all weights (fp64 accumulation), of the learned preconditioner's
- * loss 0.5/n * sum_r w_r (a_r (1 + y_r) - b_r)^2 (a = diagonal correction, b = exact correction,
- * w = sampling weight); returns the loss. */
+ * loss 0.5/n * sum_r w_r (a_r (1 + c tanh(y_r)) - b_r)^2 (a = diagonal correction, b = exact
+ * correction, w = sampling weight, c = ORC_MLP_BOUND, y = orc_mlp_forward's output); returns the
+ * loss. */
+#define ORC_MLP_BOUND 0.5
 double orc_mlp_backward(int n, int din, int dh, const float *x, const float *a, const float *b,
                         const float *w, const float *W1, const float *b1, const float *W2,
                         const float *b2, const float *W3, const float *b3, double *gW1, double *gb1,

@@ -284,10 +284,12 @@ __global__ void head_kernel(const float *__restrict__ Z2, const float *__restric
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-  const float y = part + P[ob3];
+  // bounded factor 1 + c tanh(y): the correction keeps d's sign and at most scales it by 1 +- c
+  const float th = tanhf(part + P[ob3]);
+  const float y = kMlpBound * th;
   const float A = av[s], Bv = bv[s], W = wv[s];
   const float e = A * (1.f + y) - Bv;
-  const float g = W * A * e * inv_n;
+  const float g = W * A * e * inv_n * kMlpBound * (1.f - th * th);
   if (lane == 0) {
     gy[s] = g;
     lossv[s] = 0.5f * W * e * e * inv_n;
@@ -544,7 +546,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(InferArgs a, 
       const size_t kk = tile * 128 + row;
       if (kk < a.count) {
         const size_t i = a.idx ? (size_t)__ldg(&a.idx[kk]) : kk;
-        const float y = acc + part[row] + __ldg(&a.P[ob3]);
+        const float y = kMlpBound * tanhf(acc + part[row] + __ldg(&a.P[ob3]));
         t[i] = (T)(dsh[row] * (1.0 + (double)y));
       }
     }

@@ -10,6 +10,7 @@ namespace sbdtpb {
 constexpr int kMlpHidden = SBD_TPB_MLP_HIDDEN;   // width of both hidden layers
 constexpr int kMlpFeat = SBD_TPB_MLP_FEATURES;   // input width (K of the first layer)
 constexpr int kMlpWin = 24;                      // orbitals per spin around the Fermi level
+constexpr float kMlpBound = 0.5f;                // correction factor 1 + 0.5 tanh(y) in (0.5, 1.5)
 
 // Steps of a Davidson run kept for training (FP32 copies, separated convention).  Step k: the
 // diagonal correction d_k = r_k / (E_k - H_ii), E_k, |r_k| and the indices of its orthonormal
