@@ -395,7 +395,7 @@ constexpr uint32_t kSmInfer = kSmW1 + kSmW2 + kSmA + kSmPart + kSmD + 64;
 struct InferArgs {
   const double *hii;
   const double *kxa, *kxb;  // same-spin exchange sums of the alpha / beta strings
-  double e0, inv_rnorm;
+  double e0;
   const uint32_t *occ_a, *occ_b;
   uint32_t nb;
   const uint32_t *idx;  // determinants to correct (null: all of 0 .. count-1)
@@ -589,7 +589,7 @@ struct PairArgs {
   double hd[kMaxBasis];       // P d   = d   - sum_j hd_j C_j
   int m;
   double inv_dn, alpha, c;    // 1/|d|, fit scale, sampling scale p = min(1, c (|a| + |b|))
-  double e0, inv_rnorm;
+  double e0;
   uint64_t seed;
 };
 
@@ -1012,7 +1012,6 @@ int add_step_pairs(sbd_tpb_precond *p, sbd_tpb_handle *h, const DavRecord &rec, 
     g2 += cj * cj;
   }
   a.e0 = rec.e0[k];
-  a.inv_rnorm = rec.rnorm[k] > 0.0 ? 1.0 / rec.rnorm[k] : 0.0;
   a.seed = p->seed * 0x9E3779B97F4A7C15ull + (uint64_t)(p->steps_seen++) * 0xD1B54A32D192ED03ull + 0x1234567ull;
   double *part = nullptr;
   uint8_t *flags = nullptr;
@@ -1132,7 +1131,7 @@ int precond_apply(sbd_tpb_handle *h, sbd_tpb_precond *p, T *t, double e0, double
   a.kxa = h->d_kx_a;
   a.kxb = h->d_kx_b;
   a.e0 = e0;
-  a.inv_rnorm = rnorm > 0.0 ? 1.0 / rnorm : 0.0;
+  (void)rnorm;  // the residual-entry input is held at zero (spin symmetry)
   a.occ_a = h->d_occw_a;
   a.occ_b = h->d_occw_b;
   a.nb = (uint32_t)h->bstr.size();

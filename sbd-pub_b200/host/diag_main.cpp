@@ -5,6 +5,7 @@
 // " Sample-based diagonalization: ..."), same 1pRDM.txt / 2pRDM.txt files and energy
 // decomposition (main.cc:196-319).  Extra flags select the arithmetic and the correction:
 //   --precision fp64|mixed   --preconditioner diagonal|learned   --device N
+//   --precond_params FILE    (the learned network's SBD_TPB_MLP_PARAMS FP32 values, raw)
 // --loadname / --savename read and write the reference's one-rank wavefunction file
 // (tpb/restart.h).  Flags for parts outside this build (carry-over selection,
 // --dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
@@ -30,7 +31,7 @@ namespace {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string adetfile = "alphadets.txt", bdetfile, fcidumpfile = "fcidump.txt", loadname, savename;
+  std::string adetfile = "alphadets.txt", bdetfile, fcidumpfile = "fcidump.txt", loadname, savename, precond_file;
   sbd_tpb_params prm;
   sbd_tpb_default_params(&prm);
   prm.verbose = 1;
@@ -77,6 +78,7 @@ int main(int argc, char **argv) {
       else if (v == "learned") prm.preconditioner = SBD_TPB_PRECOND_LEARNED;
       else die("--preconditioner must be diagonal or learned");
     } else if (a == "--device") prm.device = std::atoi(next().c_str());
+    else if (a == "--precond_params") precond_file = next();
     else if (a == "--use_precalculated_dets" || a == "--max_memory_gb_for_determinants" ||
              a == "--thrust_collapse_loops") next();
   }
@@ -125,9 +127,36 @@ int main(int argc, char **argv) {
               << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << " (sec) "
               << std::endl;
   }
-  const int rc = sbd_tpb_diag_from(&prm, &ham, adet.data(), na, bdet.data(), nb, W0.empty() ? nullptr : W0.data(),
-                                   &res);
-  if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(sbd_tpb_last_error());
+  int rc = SBD_TPB_OK;
+  if (prm.preconditioner == SBD_TPB_PRECOND_LEARNED) {
+    // the learned network, read from a parameter file, attached to the handle of this solve
+    if (precond_file.empty()) die("--preconditioner learned needs --precond_params FILE");
+    std::vector<float> params(SBD_TPB_MLP_PARAMS);
+    std::ifstream pf(precond_file, std::ios::binary);
+    if (!pf.read(reinterpret_cast<char *>(params.data()), sizeof(float) * params.size()))
+      die("cannot read " + std::to_string(SBD_TPB_MLP_PARAMS) + " FP32 values from " + precond_file);
+    const auto t0 = std::chrono::steady_clock::now();
+    sbd_tpb_handle *h = nullptr;
+    sbd_tpb_precond *pc = nullptr;
+    if (sbd_tpb_create(prm.device, &h) || sbd_tpb_set_hamiltonian(h, &ham) ||
+        sbd_tpb_set_strings(h, adet.data(), na, bdet.data(), nb))
+      die(sbd_tpb_last_error());
+    const auto t1 = std::chrono::steady_clock::now();
+    if (sbd_tpb_build_tables(h) || sbd_tpb_precond_create(prm.device, 0, &pc) ||
+        sbd_tpb_precond_set_params(pc, params.data(), params.size()) || sbd_tpb_set_preconditioner(h, pc))
+      die(sbd_tpb_last_error());
+    res.seconds_tables = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+    if (!prm.do_rdm) res.one_rdm = res.two_rdm = nullptr;
+    rc = sbd_tpb_davidson(h, &prm, W0.empty() ? nullptr : W0.data(), &res);
+    const std::string msg = rc == SBD_TPB_OK ? std::string() : std::string(sbd_tpb_last_error());
+    sbd_tpb_destroy(h);
+    sbd_tpb_precond_destroy(pc);
+    res.seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(msg);
+  } else {
+    rc = sbd_tpb_diag_from(&prm, &ham, adet.data(), na, bdet.data(), nb, W0.empty() ? nullptr : W0.data(), &res);
+    if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(sbd_tpb_last_error());
+  }
   if (!savename.empty() && !tpbio::save_wavefunction(savename, L, bit_length, adet, bdet, W, &err)) die(err);
   std::cout << " Elapsed time for helper construction " << res.seconds_tables << " (sec) " << std::endl;
   std::cout << " Elapsed time for davidson " << res.seconds_davidson << " (sec) " << std::endl;

@@ -90,3 +90,29 @@ def test_cli_missing_wavefunction_file(tmp_path):
                        capture_output=True, text=True, timeout=60, cwd=str(tmp_path))
     assert r.returncode != 0
 
+
+@pytest.mark.gpu
+def test_cli_learned_preconditioner_params(tmp_path):
+    """--preconditioner learned with a parameter file: an untrained network (factor 1) gives the
+    diagonal solver's energy; without a file the flag is rejected."""
+    import sbd_tpb
+    import synth
+    prob, g, meta = golden_problem("n2_1em3")
+    fcidump = str(tmp_path / "fcidump.txt")
+    alpha = str(tmp_path / "alpha.txt")
+    synth.write_fcidump(fcidump, prob.norb, prob.nelec, prob.h1, prob.eri_packed, prob.core)
+    synth.write_strings(alpha, prob.astr, prob.norb)
+    pc = sbd_tpb.Precond(0, seed=3)
+    pc.get_params().tofile(str(tmp_path / "net.bin"))
+    pc.close()
+    base = [DIAG, "--fcidump", fcidump, "--adetfile", alpha, "--iteration", "10", "--block", "10",
+            "--tolerance", "1e-8"]
+    r = subprocess.run(base + ["--preconditioner", "learned", "--precond_params", "net.bin"],
+                       capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    e = float(re.search(r"^ Energy = ([-0-9.eE+]+)", r.stdout, re.M).group(1))
+    assert e == pytest.approx(golden_cases()["n2_1em3"]["energy"], abs=1e-8)
+    r2 = subprocess.run(base + ["--preconditioner", "learned"], capture_output=True, text=True, timeout=600,
+                        cwd=str(tmp_path))
+    assert r2.returncode != 0
+
