@@ -542,7 +542,10 @@ int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
 template <typename T>
 int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, double shift) {
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
-  const bool dense_ab = h->ab.enabled;
+  // dense alpha-beta path only where the contraction runs on the tensor cores (FP32 vectors): in
+  // FP64 the shared-memory sparse kernel is faster even at full-CI connectivity (norb=12 FCI:
+  // 1.5 ms against 3.4 ms for the CUDA-core gather/contract/scatter)
+  const bool dense_ab = h->ab.enabled && sizeof(T) == 4 && h->ab.tc_ready;
   const size_t n = h->ndet();
   if (h->ct_bytes < n * sizeof(T)) {
     if (h->d_ct) cudaFree(h->d_ct);
