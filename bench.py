@@ -10,8 +10,12 @@ path has no data exchange on one node in this build): every rank solves its own 
 `value` is the aggregate.  `--impl reference` times the reference's own CPU sigma (compiled
 unchanged under oracle/_ref) on a bounded sample of the same workload with all host threads.
 
+The line also carries `carryover`: the carry-over string selection (sbd_tpb_carryover_strings,
+the step after the solve in the reference's sbd::tpb::diag) on an FP64 vector of the workload,
+with the roofline of its pass over W and the CPU restatement timed on a sample of rows.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload sci32]
-                    [--precision mixed|fp64] [--impl ours|reference] [--no-solve]
+                    [--precision mixed|fp64] [--impl ours|reference] [--no-solve] [--no-carryover]
 """
 from __future__ import annotations
 
@@ -46,6 +50,7 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
+    ap.add_argument("--no-carryover", action="store_true", help="skip the carry-over measurement")
     ap.add_argument("--davidson-cycle", action="store_true",
                     help="only run one Davidson cycle (8 sigma steps, final FP64 sigma) on the workload "
                          "and print its time; the command the Davidson launch-list profile is taken on")
@@ -263,6 +268,53 @@ def train_preconditioner(device):
                 "train_error_learned_over_diagonal": lt / dt if dt > 0 else None}
 
 
+def carryover_measure(h, prob, cpu_sample=True):
+    """Carry-over selection on an FP64 vector of the workload's size held in HBM: per-call times of
+    the pass over W (CUDA events) and of the whole call for types 1 (dominant strings) and 3
+    (singles of the determinants above a cutoff).  The pass reads W once (8 bytes per
+    determinant) and writes per-string sums: its roofline is HBM bandwidth."""
+    import torch
+
+    import sbd_tpb
+    N = prob.ndet
+    g = torch.Generator(device=f"cuda:{h.device}").manual_seed(99)
+    W = torch.randn(N, dtype=torch.float64, device=f"cuda:{h.device}", generator=g)
+    W /= torch.linalg.vector_norm(W)
+    out = {}
+    for name, kind, thr in (("dominant", sbd_tpb.CARRYOVER_DOMINANT, 0.01),
+                            ("cutoff_singles", sbd_tpb.CARRYOVER_CUTOFF_SINGLES, 1e-7)):
+        for _ in range(3):
+            r = h.carryover(W, kind, 0.0, thr, mem=sbd_tpb.DEVICE)
+        ts = []
+        for _ in range(5):
+            r = h.carryover(W, kind, 0.0, thr, mem=sbd_tpb.DEVICE)
+            ts.append(h.last_carryover_ms())
+        ts = np.array(ts)
+        pass_ms = float(np.median(ts[:, 0]))
+        pk = peaks()
+        gbs = N * 8 / (pass_ms * 1e-3) / 1e9
+        out[name] = {"pass_ms": pass_ms, "call_ms": float(np.median(ts[:, 1])), "threshold": thr,
+                     "strings_out": [len(r["astr"]), len(r["bstr"])],
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                                  "frac": gbs / pk["hbm_gbs"], "algorithmic_bytes": N * 8}}
+    if cpu_sample:
+        # the CPU restatement (oracle, one thread) of the same pass on the first rows of W
+        import pyoracle
+        na, nb = len(prob.astr), len(prob.bstr)
+        rows = max(1, min(na, int(2e7) // nb))
+        w = W[: rows * nb].cpu().numpy()
+        t0 = time.perf_counter()
+        pyoracle.string_weights(w, rows, nb)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows * nb / dt / 1e9, "unit": "GDets/s", "cores": 1, "kind": "port",
+                               "sample": f"per-string weights of the first {rows} alpha rows x {nb} "
+                                         f"(orc_string_weights, tpb/rdmat.h:11-61, 138-188)"}
+        out["gpu_pass_gdets"] = N / (out["dominant"]["pass_ms"] * 1e-3) / 1e9
+    del W
+    torch.cuda.empty_cache()
+    return out
+
+
 def time_to_solution(h, args):
     """Wall time of whole Davidson solves from the HF start: the FP64 reference answer (residual
     1e-6), then plain FP64, mixed precision and mixed precision + learned preconditioner, all to
@@ -394,6 +446,11 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.empty_cache()
         solve = time_to_solution(h, args)
 
+    carry = None
+    if not args.no_carryover and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        carry = carryover_measure(h, prob, cpu_sample=rank == 0 and not args.no_cpu)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_reference_sigma(args.workload, args.cpu_sample_seconds)
@@ -416,7 +473,7 @@ def run_ours(args, world, rank, local, pg):
                        "l2": "inputs larger than L2 (vector of %.2f GB)" % (N * esz / 1e9),
                        "tables_s": t_tables, "setup_s": t1 - t0},
             "gpu_launches": launches, "clocks": clocks.summary(), "roofline": roofline, "e2e": e2e,
-            "cpu_baseline": cpu, "time_to_solution": solve,
+            "cpu_baseline": cpu, "time_to_solution": solve, "carryover": carry,
         }
         print(json.dumps(line), flush=True)
     h.close()

@@ -35,6 +35,7 @@ extern "C" {
 #define SBD_TPB_ERR_STATE (-5)         /* call order: e.g. sigma before strings/Hamiltonian */
 #define SBD_TPB_ERR_IO (-6)            /* file could not be read or parsed */
 #define SBD_TPB_ERR_NO_DEVICE (-7)     /* no usable sm_100 device */
+#define SBD_TPB_ERR_CAPACITY (-8)      /* caller buffer missing or too small; sizes were returned */
 
 /* Memory location of caller buffers passed to the vector entry points. */
 #define SBD_TPB_HOST 0
@@ -92,6 +93,34 @@ typedef struct sbd_tpb_hamiltonian {
   size_t n_eri_packed;
 } sbd_tpb_hamiltonian;
 
+/* Carry-over strings: the step after the solver in the sample-based loop (tpb/sbdiag.h:690-736;
+ * app flags --carryover_type / --carryover_ratio / --carryover_threshold). */
+#define SBD_TPB_CARRYOVER_NONE 0
+#define SBD_TPB_CARRYOVER_DOMINANT 1         /* CarryOverAdet/Bdet (tpb/rdmat.h:63-262) */
+#define SBD_TPB_CARRYOVER_DOMINANT_SINGLES 2 /* the dominant strings and all their single
+                                                excitations, sorted and unique
+                                                (SinglesExtendHalfdets, tpb/extend.h:186-320) */
+#define SBD_TPB_CARRYOVER_CUTOFF_SINGLES 3   /* the strings of determinants with W^2 > threshold and
+                                                their singles, sorted and unique
+                                                (SinglesExtendHalfdets, tpb/extend.h:13-177) */
+
+typedef struct sbd_tpb_carryover {
+  int type;           /* SBD_TPB_CARRYOVER_* */
+  double ratio;       /* types 1, 2: > 0 keeps the first (size_t)(ratio * n) strings of each spin by
+                         descending weight; 0 keeps them up to and including the first whose running
+                         weight exceeds 1 - threshold (all of them if none does) */
+  double threshold;   /* the reference's default is 0.01 */
+  uint64_t *astr;     /* out: caller buffer (host) for the alpha strings, or NULL to query */
+  size_t acap;        /* its capacity in strings */
+  size_t na;          /* out: number of alpha strings (also when the buffer was too small) */
+  uint64_t *bstr;     /* out: the same for beta */
+  size_t bcap;
+  size_t nb;
+  double truncated_a; /* out, ratio mode: 1 - weight of the kept alpha strings */
+  double truncated_b; /* out, ratio mode: the same for beta */
+  double total_weight;/* out, type 3: weight of the determinants above the threshold */
+} sbd_tpb_carryover;
+
 /* Results; pointer fields are caller-allocated (host) and may be NULL to skip that output. */
 typedef struct sbd_tpb_result {
   double energy;      /* <W|H|W> with an FP64 sigma (tpb/sbdiag.h:431-469) */
@@ -105,6 +134,9 @@ typedef struct sbd_tpb_result {
   double seconds_tables, seconds_davidson, seconds_rdm, seconds_total;
   int learned_steps;  /* Davidson corrections taken from the learned preconditioner */
   int fallback_steps; /* steps that fell back to the diagonal after a learned step failed */
+  sbd_tpb_carryover *carryover; /* optional: with type != 0, carry-over strings of the final
+                                   vector (as sbd_tpb_carryover_strings); a buffer that is too small makes
+                                   the call return SBD_TPB_ERR_CAPACITY after everything else */
 } sbd_tpb_result;
 
 /* ---- one-shot driver: replaces sbd::tpb::diag (tpb/sbdiag.h:139-151, one rank, --method 0) */
@@ -189,6 +221,20 @@ SBD_TPB_API int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params
  * MultTPBThrust::correlation (tpb/correlation_thrust.h:504-731).  one: [2*L*L], two: [4*L^4]
  * (two may be NULL for the 1-RDM only).  W in the reference convention. */
 SBD_TPB_API int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, int mem);
+
+/* Carry-over strings of W ([na*nb], either sign convention: only W^2 enters), as sbd::tpb::diag
+ * selects them after the solve (tpb/sbdiag.h:690-736).  Strings are written to co->astr/bstr when
+ * both buffers hold them; otherwise the counts are returned in co->na/nb with
+ * SBD_TPB_ERR_CAPACITY (pass NULL buffers to query, or size them with
+ * sbd_tpb_carryover_capacity).  Strings of types 1 and 2 come out by descending weight (type 1;
+ * equal weights by ascending string index) or ascending as integers (types 2 and 3). */
+SBD_TPB_API int sbd_tpb_carryover_strings(sbd_tpb_handle *h, const double *W, int mem, sbd_tpb_carryover *co);
+/* Upper bound of the strings one spin (0 alpha, 1 beta) can produce for a carry-over type. */
+SBD_TPB_API size_t sbd_tpb_carryover_capacity(sbd_tpb_handle *h, int type, int spin);
+/* Times of the last carry-over on the handle, milliseconds: [0] the pass over W that forms the
+ * per-string weights or counts (CUDA events on the handle's stream), [1] the whole call (host
+ * clock, including sorting, extension and copies). */
+SBD_TPB_API int sbd_tpb_last_carryover_ms(sbd_tpb_handle *h, double *ms);
 
 /* Device stream of the handle (cudaStream_t as void*), for callers that order their own work. */
 SBD_TPB_API void *sbd_tpb_stream(sbd_tpb_handle *h);

@@ -79,6 +79,13 @@ def lib():
         L.orc_reorder_sign.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                       _f32p, _f32p, _f32p, _f32p]
+        L.orc_string_weights.argtypes = [_f64p, C.c_size_t, C.c_size_t, C.c_double, _f64p, _f64p, _u64p, _u64p,
+                                         C.POINTER(C.c_double)]
+        L.orc_carryover_select.restype = C.c_size_t
+        L.orc_carryover_select.argtypes = [_f64p, C.c_size_t, C.c_double, C.c_double, _u64p,
+                                           C.POINTER(C.c_double)]
+        L.orc_singles_extend.restype = C.c_size_t
+        L.orc_singles_extend.argtypes = [_u64p, C.c_size_t, C.c_int, _u64p]
         L.orc_mlp_backward.restype = C.c_double
         L.orc_mlp_backward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                        _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
@@ -230,6 +237,59 @@ class System:
 
 def reorder_sign(a: int, b: int) -> int:
     return lib().orc_reorder_sign(int(a), int(b))
+
+
+def string_weights(W: np.ndarray, na: int, nb: int, cutoff: float = 0.0):
+    """(wa, wb, ca, cb, total): per-string weights of W and the counts/total above the cutoff
+    (orc_string_weights)."""
+    W = np.ascontiguousarray(W, np.float64).reshape(-1)
+    wa, wb = np.zeros(na), np.zeros(nb)
+    ca, cb = np.zeros(na, np.uint64), np.zeros(nb, np.uint64)
+    t = C.c_double(0.0)
+    lib().orc_string_weights(W, na, nb, float(cutoff), wa, wb, ca, cb, C.byref(t))
+    return wa, wb, ca, cb, t.value
+
+
+def carryover_select(w: np.ndarray, ratio: float, threshold: float):
+    """(order[:kept], truncated weight) of the dominant strings (orc_carryover_select)."""
+    w = np.ascontiguousarray(w, np.float64)
+    order = np.zeros(len(w), np.uint64)
+    t = C.c_double(0.0)
+    k = lib().orc_carryover_select(w, len(w), float(ratio), float(threshold), order, C.byref(t))
+    return order[:k].astype(np.int64), t.value
+
+
+def singles_extend(s: np.ndarray, L: int) -> np.ndarray:
+    """Strings plus all their single excitations, sorted and unique (orc_singles_extend)."""
+    s = np.ascontiguousarray(s, np.uint64)
+    if len(s) == 0:
+        return s.copy()
+    e = int(bin(int(s[0])).count("1"))
+    out = np.zeros(len(s) * (1 + e * (L - e)), np.uint64)
+    m = lib().orc_singles_extend(s, len(s), L, out)
+    return out[:m].copy()
+
+
+def carryover(W: np.ndarray, astr: np.ndarray, bstr: np.ndarray, L: int, kind: int, ratio: float,
+              threshold: float):
+    """Carry-over strings of W as the reference's sbd::tpb::diag computes them (tpb/sbdiag.h:690-736):
+    kind 1 = dominant strings, 2 = dominant strings and their singles, 3 = singles of the strings in
+    determinants with W^2 > threshold.  Returns (co_a, co_b, truncated_a, truncated_b, total)."""
+    na, nb = len(astr), len(bstr)
+    if kind in (1, 2):
+        wa, wb, _, _, _ = string_weights(W, na, nb)
+        oa, ta = carryover_select(wa, ratio, threshold)
+        ob, tb = carryover_select(wb, ratio, threshold)
+        co_a, co_b = np.asarray(astr, np.uint64)[oa], np.asarray(bstr, np.uint64)[ob]
+        if kind == 2:
+            co_a, co_b = singles_extend(co_a, L), singles_extend(co_b, L)
+        return co_a, co_b, ta, tb, 0.0
+    if kind == 3:
+        _, _, ca, cb, total = string_weights(W, na, nb, threshold)
+        co_a = singles_extend(np.asarray(astr, np.uint64)[ca > 0], L)
+        co_b = singles_extend(np.asarray(bstr, np.uint64)[cb > 0], L)
+        return co_a, co_b, 0.0, 0.0, total
+    raise ValueError("carry-over kind must be 1, 2 or 3")
 
 
 def _f32(x):

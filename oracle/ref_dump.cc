@@ -14,9 +14,19 @@
 //   davidson.txt / W.f64  Davidson (tpb/davidson.h:667-930) from the HF start, energy as in
 //                         tpb/sbdiag.h:431-469
 //   rdm1.f64 / rdm2.f64   Correlation (tpb/correlation.h:378-664)
+//   co<k>_{a,b}.u64, carryover.txt   carry-over strings of W (tpb/sbdiag.h:690-736):
+//                         co1 = CarryOverAdet/Bdet with the threshold (tpb/rdmat.h:63-100,
+//                         190-227), co1r = the same with n_kept = ratio * size (:102-135,
+//                         229-262) and its truncated weights, co2 = SinglesExtendHalfdets of co1
+//                         (tpb/extend.h:186-320), co3 = SinglesExtendHalfdets(W, ..., cutoff)
+//                         (tpb/extend.h:13-177) and its total weight.  co2 and co3 only when both
+//                         spins hold the same number of electrons: for unequal counts the
+//                         reference sizes the beta arrays from the alpha count (extend.h:85, 222,
+//                         248-249), so co2 throws std::out_of_range and co3 broadcasts empty
+//                         trailing strings (a null dereference in MpiBcast)
 //
 // Usage: ref_dump --fcidump F --adetfile A [--bdetfile B] [--bit_length 20] --out DIR
-//                 [--sigma_seed S] [--davidson IT NB TOL] [--rdm]
+//                 [--sigma_seed S] [--davidson IT NB TOL] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
 // The reference headers rely on their includer for these (as its app main.cc does).
 #include <chrono>
 #include <cmath>
@@ -82,6 +92,7 @@ int main(int argc, char **argv) {
   int dav_it = 0, dav_nb = 0;
   double dav_tol = 1e-8;
   bool do_rdm = false;
+  double co_ratio = -1.0, co_threshold = 0.0, co_cutoff = 0.0;
   for (int i = 1; i < argc; ++i) {
     std::string a(argv[i]);
     if (a == "--fcidump") fcidumpfile = argv[++i];
@@ -95,6 +106,11 @@ int main(int argc, char **argv) {
       dav_nb = std::atoi(argv[++i]);
       dav_tol = std::atof(argv[++i]);
     } else if (a == "--rdm") do_rdm = true;
+    else if (a == "--carryover") {
+      co_ratio = std::atof(argv[++i]);
+      co_threshold = std::atof(argv[++i]);
+      co_cutoff = std::atof(argv[++i]);
+    }
   }
   int provided;
   MPI_Init_thread(&argc, &argv, MPI_THREAD_FUNNELED, &provided);
@@ -195,6 +211,39 @@ int main(int argc, char **argv) {
       for (auto &v : two) r2.insert(r2.end(), v.begin(), v.end());
       write_raw(out + "/rdm1.f64", r1.data(), r1.size());
       write_raw(out + "/rdm2.f64", r2.data(), r2.size());
+    }
+    if (co_ratio >= 0.0) {
+      auto dump = [&](const std::string &name, const std::vector<std::vector<size_t>> &d) {
+        auto p = pack_strings(d, bit_length, L);
+        write_raw(out + "/" + name + ".u64", p.data(), p.size());
+      };
+      std::vector<std::vector<size_t>> co_a, co_b, ex_a, ex_b;
+      sbd::CarryOverAdet(W, adet, bdet, 1, 1, b_comm, co_a, co_threshold);
+      sbd::CarryOverBdet(W, adet, bdet, 1, 1, b_comm, co_b, co_threshold);
+      dump("co1_a", co_a);
+      dump("co1_b", co_b);
+      const bool same_count = sbd::bitcount(adet[0], bit_length, L) == sbd::bitcount(bdet[0], bit_length, L);
+      if (same_count) {
+        sbd::SinglesExtendHalfdets(co_a, co_b, bit_length, static_cast<size_t>(L), 1, 1, b_comm, ex_a, ex_b);
+        dump("co2_a", ex_a);
+        dump("co2_b", ex_b);
+      }
+      double tw_a = 0.0, tw_b = 0.0, total = 0.0;
+      std::vector<std::vector<size_t>> cr_a, cr_b;
+      sbd::CarryOverAdet(W, adet, bdet, 1, 1, b_comm, static_cast<size_t>(co_ratio * adet.size()), cr_a, tw_a);
+      sbd::CarryOverBdet(W, adet, bdet, 1, 1, b_comm, static_cast<size_t>(co_ratio * bdet.size()), cr_b, tw_b);
+      dump("co1r_a", cr_a);
+      dump("co1r_b", cr_b);
+      if (same_count) {
+        std::vector<std::vector<size_t>> c3_a, c3_b;
+        sbd::SinglesExtendHalfdets(W, adet, bdet, bit_length, static_cast<size_t>(L), 1, 1, b_comm,
+                                   co_cutoff, c3_a, c3_b, total);
+        dump("co3_a", c3_a);
+        dump("co3_b", c3_b);
+      }
+      std::ofstream oc(out + "/carryover.txt");
+      oc.precision(17);
+      oc << co_ratio << " " << co_threshold << " " << co_cutoff << " " << tw_a << " " << tw_b << " " << total << "\n";
     }
   }
   MPI_Finalize();

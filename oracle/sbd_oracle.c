@@ -909,3 +909,91 @@ double orc_mlp_backward(int n, int din, int dh, const float *x, const float *a, 
   free(y);
   return loss;
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Carry-over strings (tpb/sbdiag.h:690-736, tpb/rdmat.h, tpb/extend.h)                        */
+/* ------------------------------------------------------------------------------------------ */
+
+void orc_string_weights(const double *W, size_t na, size_t nb, double cutoff, double *wa, double *wb,
+                        uint64_t *ca, uint64_t *cb, double *total) {
+  /* DiagonalAdetReducedDensityMatrix (tpb/rdmat.h:47-54): ib inner, in order */
+  for (size_t ia = 0; ia < na; ia++) {
+    double d = 0.0;
+    for (size_t ib = 0; ib < nb; ib++) d += W[ia * nb + ib] * W[ia * nb + ib];
+    wa[ia] = d;
+  }
+  /* DiagonalBdetReducedDensityMatrix (tpb/rdmat.h:174-181): ia inner, in order */
+  for (size_t ib = 0; ib < nb; ib++) {
+    double d = 0.0;
+    for (size_t ia = 0; ia < na; ia++) d += W[ia * nb + ib] * W[ia * nb + ib];
+    wb[ib] = d;
+  }
+  /* SinglesExtendHalfdets (tpb/extend.h:45-58): counts above the cutoff, their total weight */
+  if (ca) memset(ca, 0, sizeof(uint64_t) * na);
+  if (cb) memset(cb, 0, sizeof(uint64_t) * nb);
+  double t = 0.0;
+  for (size_t ia = 0; ia < na; ia++)
+    for (size_t ib = 0; ib < nb; ib++) {
+      const double x = W[ia * nb + ib] * W[ia * nb + ib];
+      if (x > cutoff) {
+        t += x;
+        if (ca) ca[ia]++;
+        if (cb) cb[ib]++;
+      }
+    }
+  if (total) *total = t;
+}
+
+static const double *g_sel_w; /* weights seen by the comparator below */
+
+static int cmp_weight_desc(const void *x, const void *y) {
+  const size_t i = *(const size_t *)x, j = *(const size_t *)y;
+  if (g_sel_w[i] > g_sel_w[j]) return -1;
+  if (g_sel_w[i] < g_sel_w[j]) return 1;
+  return (i > j) - (i < j);
+}
+
+size_t orc_carryover_select(const double *w, size_t n, double ratio, double threshold, size_t *order,
+                            double *truncated) {
+  for (size_t i = 0; i < n; i++) order[i] = i;
+  g_sel_w = w;
+  qsort(order, n, sizeof(size_t), cmp_weight_desc); /* tpb/rdmat.h:78-83 */
+  if (ratio > 0.0) {
+    /* n_kept = static_cast<size_t>(ratio * size) (tpb/sbdiag.h:703), weight summed in order */
+    size_t kept = (size_t)(ratio * (double)n);
+    if (kept > n) kept = n;
+    double sum = 0.0;
+    for (size_t i = 0; i < kept; i++) sum += w[order[i]];
+    if (truncated) *truncated = 1.0 - sum;
+    return kept;
+  }
+  /* running sums S, Imax = upper_bound(S, 1 - threshold) + 1 (tpb/rdmat.h:85-95) */
+  const double target = 1.0 - threshold;
+  double sum = 0.0;
+  size_t le = 0;
+  for (size_t i = 0; i < n; i++) {
+    sum += w[order[i]];
+    if (sum <= target) le = i + 1;
+  }
+  if (truncated) *truncated = 0.0;
+  return le + 1 < n ? le + 1 : n;
+}
+
+size_t orc_singles_extend(const uint64_t *s, size_t n, int L, uint64_t *out) {
+  size_t m = 0;
+  for (size_t i = 0; i < n; i++) out[m++] = s[i];
+  for (size_t i = 0; i < n; i++) {
+    /* single_from_hdet (basic/excitation.h:9-29): remove closed j, add open k */
+    for (int j = 0; j < L; j++) {
+      if (!((s[i] >> j) & 1)) continue;
+      const uint64_t base = s[i] & ~((uint64_t)1 << j);
+      for (int k = 0; k < L; k++)
+        if (!((s[i] >> k) & 1)) out[m++] = base | ((uint64_t)1 << k);
+    }
+  }
+  qsort(out, m, sizeof(uint64_t), cmp_u64);
+  size_t u = 0;
+  for (size_t i = 0; i < m; i++)
+    if (u == 0 || out[i] != out[u - 1]) out[u++] = out[i];
+  return u;
+}

@@ -114,6 +114,27 @@ void orc_rdm_energy(const orc_ham *h, const double *one, const double *two, doub
  * determinant (a, b): +1 or -1.  Used by tests to relate the two conventions. */
 int orc_reorder_sign(uint64_t a, uint64_t b);
 
+/* Carry-over strings of a CI vector (tpb/sbdiag.h:690-736).
+ * orc_string_weights: wa[ia] = sum over ib of W^2 and wb[ib] = sum over ia of W^2, each summed
+ * in the reference's loop order (tpb/rdmat.h:47-54, 174-181); ca/cb (may be NULL) count the
+ * entries with W^2 > cutoff per row/column and *total (may be NULL) sums those entries in
+ * row-major order (tpb/extend.h:45-58). */
+void orc_string_weights(const double *W, size_t na, size_t nb, double cutoff, double *wa, double *wb,
+                        uint64_t *ca, uint64_t *cb, double *total);
+/* Dominant strings (CarryOverAdet/Bdet, tpb/rdmat.h:63-135, 190-262): order[] receives the
+ * string indices by descending weight (equal weights by ascending index: the reference leaves
+ * their order to std::sort).  ratio > 0 keeps floor(ratio * n) strings and sets *truncated to
+ * 1 - their weight; otherwise the strings up to and including the first whose running weight
+ * exceeds 1 - threshold are kept (all n when none does: the reference then reads past its
+ * arrays).  Returns the number kept. */
+size_t orc_carryover_select(const double *w, size_t n, double ratio, double threshold, size_t *order,
+                            double *truncated);
+/* Each string of s followed by its single excitations (closed orbital j ascending, then open
+ * orbital k ascending: basic/excitation.h:9-29), then sorted ascending and made unique
+ * (SinglesExtendHalfdets, tpb/extend.h:186-320; sort_bitarray).  out needs n*(1 + e*(L-e))
+ * entries (e = electrons of the string); returns the number written. */
+size_t orc_singles_extend(const uint64_t *s, size_t n, int L, uint64_t *out);
+
 /* Tiny MLP reference for the learned preconditioner checks (see the product's mlp kernels):
  * y = W3 gelu(W2 gelu(W1 x + b1) + b2) + b3 with fp32 math; weights row-major [out][in]. */
 void orc_mlp_forward(int n, int din, int dh, const float *x, const float *W1, const float *b1,

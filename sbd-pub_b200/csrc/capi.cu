@@ -108,6 +108,7 @@ int sbd_tpb_create(int device, sbd_tpb_handle **out) {
   h->smem_optin = prop.sharedMemPerBlockOptin;
   bool ev_ok = cudaEventCreate(&h->ev0) == cudaSuccess && cudaEventCreate(&h->ev1) == cudaSuccess;
   for (cudaEvent_t &e : h->ev_k) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+  for (cudaEvent_t &e : h->ev_co) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess || !ev_ok) {
     delete h;
     return fail(SBD_TPB_ERR_CUDA, "stream/event creation failed");
@@ -124,6 +125,8 @@ int sbd_tpb_destroy(sbd_tpb_handle *h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   for (cudaEvent_t e : h->ev_k)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->ev_co)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -354,6 +357,36 @@ int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, in
   }
   TPB_CUDA(cudaStreamSynchronize(h->stream));
   return rdm_sep(h, h->d_tmp64, one, two, nullptr);
+}
+
+int sbd_tpb_carryover_strings(sbd_tpb_handle *h, const double *W, int mem, sbd_tpb_carryover *co) {
+  TPB_HANDLE(h);
+  if (!h->have_strings) return fail(SBD_TPB_ERR_STATE, "strings not set");
+  if (!W || !co) return fail(SBD_TPB_ERR_INVALID, "null vector/carry-over record");
+  if (mem == SBD_TPB_DEVICE) return carryover_device(h, W, co);
+  TPB_CHECK(ensure_tmp64(h));
+  TPB_CUDA(cudaMemcpyAsync(h->d_tmp64, W, sizeof(double) * h->ndet(), cudaMemcpyHostToDevice, h->stream));
+  return carryover_device(h, h->d_tmp64, co);
+}
+
+int sbd_tpb_last_carryover_ms(sbd_tpb_handle *h, double *ms) {
+  if (!h || !ms) return fail(SBD_TPB_ERR_INVALID, "null handle/output");
+  ms[0] = h->last_carryover_ms[0];
+  ms[1] = h->last_carryover_ms[1];
+  return SBD_TPB_OK;
+}
+
+size_t sbd_tpb_carryover_capacity(sbd_tpb_handle *h, int type, int spin) {
+  if (!h || !h->have_strings) return 0;
+  const size_t n = spin ? h->bstr.size() : h->astr.size();
+  if (type == SBD_TPB_CARRYOVER_DOMINANT) return n;
+  if (type != SBD_TPB_CARRYOVER_DOMINANT_SINGLES && type != SBD_TPB_CARRYOVER_CUTOFF_SINGLES) return 0;
+  // every string and its e(L - e) singles, at most C(L, e) distinct strings
+  const int L = h->L, e = spin ? h->n_beta : h->n_alpha;
+  double binom = 1.0;
+  for (int k = 1; k <= e; k++) binom = binom * (L - e + k) / k;
+  const double bound = std::min((double)n * (1.0 + (double)e * (L - e)), std::floor(binom + 0.5));
+  return (size_t)bound;
 }
 
 int sbd_tpb_diag(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *ham,

@@ -439,11 +439,19 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
     if (res->one_rdm || res->two_rdm) pool_clear(h);  // the 2-RDM passes need their own N-vectors
     TPB_CHECK(rdm_sep(h, dW.p, res->one_rdm, res->two_rdm, res->density));
   }
+  // carry-over strings of the final vector (tpb/sbdiag.h:690-736); a short caller buffer is
+  // reported after the rest of the result is filled
+  int co_rc = SBD_TPB_OK;
+  if (res->carryover && res->carryover->type != SBD_TPB_CARRYOVER_NONE) {
+    co_rc = carryover_device(h, dW.p, res->carryover);
+    if (co_rc != SBD_TPB_OK && co_rc != SBD_TPB_ERR_CAPACITY) return co_rc;
+  }
   res->energy = E;
   res->residual = (p->precision == SBD_TPB_MIXED) ? std::sqrt(rr) : resid;
   res->iterations = nsig;
   res->converged = conv;
   res->seconds_davidson = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (co_rc != SBD_TPB_OK) return co_rc;
   return conv ? SBD_TPB_OK : SBD_TPB_ERR_NOT_CONVERGED;
 }
 

@@ -122,6 +122,8 @@ struct sbd_tpb_handle {
   uint64_t launches = 0;
   float last_sigma_ms = 0.f;
   int sigma_kernels = 0;  // kernels timed in the last sigma (ev0, ev_k[0..], ev1)
+  cudaEvent_t ev_co[2] = {nullptr, nullptr};  // around the weight pass of the last carry-over
+  float last_carryover_ms[2] = {0.f, 0.f};    // weight pass, whole call
   int num_sms = 148;
   size_t smem_optin = 0;
 
@@ -180,6 +182,8 @@ struct sbd_tpb_handle {
 };
 
 namespace sbdtpb {
+// carryover.cu: carry-over strings of a device vector (either sign convention)
+int carryover_device(sbd_tpb_handle *h, const double *dW, sbd_tpb_carryover *co);
 // tables.cu
 int build_excitation_tables(sbd_tpb_handle *h);
 int copy_table_reference_layout(sbd_tpb_handle *h, int kind, uint64_t *off, uint64_t *ket,

@@ -7,8 +7,11 @@
 //   --precision fp64|mixed   --preconditioner diagonal|learned   --device N
 //   --precond_params FILE    (the learned network's SBD_TPB_MLP_PARAMS FP32 values, raw)
 // --loadname / --savename read and write the reference's one-rank wavefunction file
-// (tpb/restart.h).  Flags for parts outside this build (carry-over selection,
-// --dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
+// (tpb/restart.h); --carryover_type 1/2/3 with --carryover_ratio / --carryover_threshold selects
+// the carry-over strings on the GPU (tpb/sbdiag.h:690-736) and --carryover_adetfile /
+// --carryover_bdetfile write them (main.cc:203-224).  Flags for parts outside this build
+// (--dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -28,6 +31,16 @@ namespace {
   std::exit(1);
 }
 
+// most strings one spin can produce for a carry-over type: the strings themselves (type 1), or
+// every string and its singles, at most C(L, e) distinct ones (types 2, 3)
+size_t carryover_capacity(int type, int L, const std::vector<uint64_t> &s) {
+  if (type == SBD_TPB_CARRYOVER_DOMINANT || s.empty()) return s.size();
+  const int e = __builtin_popcountll(s[0]);
+  double binom = 1.0;
+  for (int k = 1; k <= e; k++) binom = binom * (L - e + k) / k;
+  return (size_t)std::min((double)s.size() * (1.0 + (double)e * (L - e)), binom + 0.5);
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -36,6 +49,8 @@ int main(int argc, char **argv) {
   sbd_tpb_default_params(&prm);
   prm.verbose = 1;
   int do_shuffle = 0, method = 0, carryover_type = 0, comm_sizes = 1;
+  double carryover_ratio = 0.0, carryover_threshold = 0.01;  // tpb/sbdiag.h:37-39
+  std::string carryover_adetfile, carryover_bdetfile;
   size_t bit_length = 20;
   std::string unsupported;
   for (int i = 1; i < argc; i++) {
@@ -58,8 +73,10 @@ int main(int argc, char **argv) {
     else if (a == "--rdm") prm.do_rdm = std::atoi(next().c_str());
     else if (a == "--bit_length") bit_length = std::strtoul(next().c_str(), nullptr, 10);
     else if (a == "--carryover_type") carryover_type = std::atoi(next().c_str());
-    else if (a == "--carryover_ratio" || a == "--carryover_threshold" ||
-             a == "--carryover_adetfile" || a == "--carryover_bdetfile") next();
+    else if (a == "--carryover_ratio") carryover_ratio = std::atof(next().c_str());
+    else if (a == "--carryover_threshold") carryover_threshold = std::atof(next().c_str());
+    else if (a == "--carryover_adetfile") carryover_adetfile = next();
+    else if (a == "--carryover_bdetfile") carryover_bdetfile = next();
     else if (a == "--adet_comm_size" || a == "--bdet_comm_size" || a == "--task_comm_size")
       comm_sizes *= std::atoi(next().c_str());
     else if (a == "--loadname") loadname = next();
@@ -86,7 +103,7 @@ int main(int argc, char **argv) {
   if (method != 0) die("only --method 0 (matrix-free Davidson) is built");
   if (comm_sizes != 1) die("one rank on one GPU: --*_comm_size must be 1");
   if (prm.init != 0) die("only --init 0 (start from the first determinant) is built");
-  if (carryover_type != 0) die("carry-over string selection is not built (--carryover_type 0)");
+  if (carryover_type < 0 || carryover_type > 3) die("--carryover_type must be 0, 1, 2 or 3");
   if (!unsupported.empty()) die("not built in this version:" + unsupported);
 
   std::cout.precision(16);
@@ -116,6 +133,22 @@ int main(int argc, char **argv) {
   res.density = density.data();
   res.one_rdm = prm.do_rdm ? one.data() : nullptr;
   res.two_rdm = prm.do_rdm ? two.data() : nullptr;
+  // carry-over strings of the final vector, selected on the GPU inside the solve
+  sbd_tpb_carryover co;
+  std::memset(&co, 0, sizeof(co));
+  std::vector<uint64_t> co_a, co_b;
+  if (carryover_type != 0) {
+    co.type = carryover_type;
+    co.ratio = carryover_ratio;
+    co.threshold = carryover_threshold;
+    co_a.resize(std::max<size_t>(1, carryover_capacity(carryover_type, L, adet)));
+    co_b.resize(std::max<size_t>(1, carryover_capacity(carryover_type, L, bdet)));
+    co.astr = co_a.data();
+    co.acap = co_a.size();
+    co.bstr = co_b.data();
+    co.bcap = co_b.size();
+    res.carryover = &co;
+  }
   // initial vector: HF determinant, or a stored wavefunction (tpb/sbdiag.h:280-296)
   std::vector<double> W0;
   if (!loadname.empty()) {
@@ -158,6 +191,14 @@ int main(int argc, char **argv) {
     if (rc != SBD_TPB_OK && rc != SBD_TPB_ERR_NOT_CONVERGED) die(sbd_tpb_last_error());
   }
   if (!savename.empty() && !tpbio::save_wavefunction(savename, L, bit_length, adet, bdet, W, &err)) die(err);
+  co_a.resize(co.na);
+  co_b.resize(co.nb);
+  if ((carryover_type == 1 || carryover_type == 2) && carryover_ratio != 0.0) {
+    std::cout << " truncated weight in carry-over for alpha-det = " << co.truncated_a << std::endl;
+    std::cout << " truncated weight in carry-over for beta-det = " << co.truncated_b << std::endl;
+  } else if (carryover_type == 3) {
+    std::cout << " percentage of wf used in augmentation: " << co.total_weight * 100.0 << std::endl;
+  }
   std::cout << " Elapsed time for helper construction " << res.seconds_tables << " (sec) " << std::endl;
   std::cout << " Elapsed time for davidson " << res.seconds_davidson << " (sec) " << std::endl;
   std::cout << " Energy = " << res.energy << std::endl;
@@ -165,7 +206,19 @@ int main(int argc, char **argv) {
   std::cout << " Sample-based diagonalization: density = ";
   for (int i = 0; i < L; i++) std::cout << ((i == 0) ? "[" : ",") << density[2 * i] + density[2 * i + 1];
   std::cout << std::endl;
-  std::cout << " Sample-based diagonalization: carryover bitstrings = [], size = 0" << std::endl;
+  std::cout << " Sample-based diagonalization: carryover bitstrings = [";
+  for (size_t i = 0; i < std::min<size_t>(co_a.size(), 4); i++)
+    std::cout << (i == 0 ? "" : ", ") << tpbio::make_string(co_a[i], L);
+  if (co_a.size() > 4) std::cout << " ..., " << tpbio::make_string(co_a.back(), L);
+  std::cout << "], size = " << co_a.size() << std::endl;
+  // carry-over files: one string per line (main.cc:213-224)
+  for (int spin = 0; spin < 2; spin++) {
+    const std::string &f = spin ? carryover_bdetfile : carryover_adetfile;
+    if (f.empty()) continue;
+    std::ofstream os(f);
+    if (!os) die("cannot write " + f);
+    for (uint64_t x : spin ? co_b : co_a) os << tpbio::make_string(x, L) << "\n";
+  }
   if (prm.do_rdm) {
     // 1pRDM.txt / 2pRDM.txt and the energy decomposition (main.cc:264-317)
     const size_t L2 = (size_t)L * L, L4 = L2 * L2;

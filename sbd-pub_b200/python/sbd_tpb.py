@@ -42,8 +42,11 @@ EXPORTED = [
     "sbd_tpb_precond_create", "sbd_tpb_precond_destroy", "sbd_tpb_precond_collect",
     "sbd_tpb_precond_num_samples", "sbd_tpb_precond_train", "sbd_tpb_precond_evaluate",
     "sbd_tpb_precond_get_params", "sbd_tpb_precond_set_params", "sbd_tpb_precond_gradients",
-    "sbd_tpb_precond_apply", "sbd_tpb_set_preconditioner",
+    "sbd_tpb_precond_apply", "sbd_tpb_set_preconditioner", "sbd_tpb_carryover_strings",
+    "sbd_tpb_carryover_capacity", "sbd_tpb_last_carryover_ms",
 ]
+CARRYOVER_NONE, CARRYOVER_DOMINANT, CARRYOVER_DOMINANT_SINGLES, CARRYOVER_CUTOFF_SINGLES = 0, 1, 2, 3
+ERR_CAPACITY = -8
 MLP_HIDDEN, MLP_FEATURES, MLP_PARAMS = 256, 64, 82689
 
 
@@ -69,6 +72,15 @@ class Hamiltonian(C.Structure):
     ]
 
 
+class Carryover(C.Structure):
+    _fields_ = [
+        ("type", C.c_int), ("ratio", C.c_double), ("threshold", C.c_double),
+        ("astr", C.POINTER(C.c_uint64)), ("acap", C.c_size_t), ("na", C.c_size_t),
+        ("bstr", C.POINTER(C.c_uint64)), ("bcap", C.c_size_t), ("nb", C.c_size_t),
+        ("truncated_a", C.c_double), ("truncated_b", C.c_double), ("total_weight", C.c_double),
+    ]
+
+
 class Result(C.Structure):
     _fields_ = [
         ("energy", C.c_double), ("residual", C.c_double), ("iterations", C.c_int),
@@ -77,6 +89,7 @@ class Result(C.Structure):
         ("two_rdm", C.POINTER(C.c_double)), ("seconds_tables", C.c_double),
         ("seconds_davidson", C.c_double), ("seconds_rdm", C.c_double),
         ("seconds_total", C.c_double), ("learned_steps", C.c_int), ("fallback_steps", C.c_int),
+        ("carryover", C.POINTER(Carryover)),
     ]
 
 
@@ -132,6 +145,10 @@ def lib():
                                             C.POINTER(C.c_double), vp]
     L.sbd_tpb_precond_apply.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp]
     L.sbd_tpb_set_preconditioner.argtypes = [vp, vp]
+    L.sbd_tpb_carryover_strings.argtypes = [vp, vp, C.c_int, C.POINTER(Carryover)]
+    L.sbd_tpb_carryover_capacity.restype = C.c_size_t
+    L.sbd_tpb_carryover_capacity.argtypes = [vp, C.c_int, C.c_int]
+    L.sbd_tpb_last_carryover_ms.argtypes = [vp, C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -275,7 +292,9 @@ class Handle:
         return lib().sbd_tpb_stream(self.h) or 0
 
     def davidson(self, params: Params | None = None, W0: np.ndarray | None = None,
-                 want_vector=True, want_rdm=False):
+                 want_vector=True, want_rdm=False, carryover: tuple | None = None):
+        """Davidson on the handle's problem; carryover = (type, ratio, threshold) also returns the
+        carry-over strings of the final vector under "carryover"."""
         prob = self.problem
         params = params or default_params()
         res = Result()
@@ -288,6 +307,10 @@ class Handle:
         res.density = dens.ctypes.data_as(dp)
         res.one_rdm = one.ctypes.data_as(dp) if one is not None else dp()
         res.two_rdm = two.ctypes.data_as(dp) if two is not None else dp()
+        co = bufs = None
+        if carryover is not None:
+            co, bufs = self._carryover_record(*carryover)
+            res.carryover = C.pointer(co)
         w0 = None if W0 is None else np.ascontiguousarray(W0, np.float64)
         rc = lib().sbd_tpb_davidson(self.h, C.byref(params), w0.ctypes.data if w0 is not None else None,
                                     C.byref(res))
@@ -295,12 +318,48 @@ class Handle:
         return dict(energy=res.energy, residual=res.residual, iterations=res.iterations,
                     converged=bool(res.converged), W=W, density=dens, one=one, two=two,
                     seconds=res.seconds_davidson, learned_steps=res.learned_steps,
-                    fallback_steps=res.fallback_steps)
+                    fallback_steps=res.fallback_steps,
+                    carryover=self._carryover_result(co, bufs) if co is not None else None)
 
     def set_preconditioner(self, pc: "Precond | None"):
         """Attach a learned preconditioner (used when params.preconditioner == PRECOND_LEARNED)."""
         _check(lib().sbd_tpb_set_preconditioner(self.h, pc.p if pc is not None else None))
         self._pc = pc  # keep it alive while attached
+
+    def _carryover_record(self, kind: int, ratio: float, threshold: float):
+        co = Carryover(type=kind, ratio=ratio, threshold=threshold)
+        bufs = []
+        for spin, (pf, cf) in enumerate((("astr", "acap"), ("bstr", "bcap"))):
+            cap = int(lib().sbd_tpb_carryover_capacity(self.h, kind, spin))
+            buf = np.zeros(max(cap, 1), np.uint64)
+            setattr(co, pf, buf.ctypes.data_as(C.POINTER(C.c_uint64)))
+            setattr(co, cf, cap)
+            bufs.append(buf)
+        return co, bufs
+
+    @staticmethod
+    def _carryover_result(co, bufs):
+        return dict(astr=bufs[0][:co.na].copy(), bstr=bufs[1][:co.nb].copy(), truncated_a=co.truncated_a,
+                    truncated_b=co.truncated_b, total_weight=co.total_weight)
+
+    def carryover(self, W, kind: int, ratio: float = 0.0, threshold: float = 0.01, mem: int = HOST):
+        """Carry-over strings of W (sbd_tpb_carryover_strings): dict with astr, bstr, truncated_a/b,
+        total_weight.  W is a host array or, with mem=DEVICE, a device tensor/pointer."""
+        co, bufs = self._carryover_record(kind, ratio, threshold)
+        if mem == HOST:
+            w = np.ascontiguousarray(W, np.float64)
+            assert w.size == self.problem.ndet
+            ptr = w.ctypes.data
+        else:
+            ptr = W if isinstance(W, int) else W.data_ptr()
+        _check(lib().sbd_tpb_carryover_strings(self.h, ptr, mem, C.byref(co)))
+        return self._carryover_result(co, bufs)
+
+    def last_carryover_ms(self):
+        """(weight pass ms, whole call ms) of the last carry-over on this handle."""
+        ms = (C.c_double * 2)()
+        _check(lib().sbd_tpb_last_carryover_ms(self.h, ms))
+        return float(ms[0]), float(ms[1])
 
     def rdm(self, W: np.ndarray, two_body=True):
         L = self.problem.norb

@@ -48,8 +48,13 @@ CASES = {
     "h2o_1em3": dict(fcidump=f"{REF}/data/h2o/fcidump.txt", adet=f"{REF}/data/h2o/h2o-1em3-alpha.txt",
                      davidson=(10, 10, 1e-8), rdm=False, full=False,
                      published=-76.23594663, published_src="data/h2o/README.md:6"),
-    "syn8": dict(synthetic=(8, 3, 3, 56, 56, 11), davidson=(10, 10, 1e-10), rdm=True, full=True),
-    "syn10_ab": dict(synthetic=(10, 4, 3, 120, 90, 23), davidson=(10, 10, 1e-10), rdm=True, full=True),
+    # carryover = (ratio, threshold, cutoff) of the carry-over dumps (ref_dump --carryover)
+    "syn8": dict(synthetic=(8, 3, 3, 56, 56, 11), davidson=(10, 10, 1e-10), rdm=True, full=True,
+                 carryover=(0.5, 0.01, 1e-3)),
+    "syn10_ab": dict(synthetic=(10, 4, 3, 120, 90, 23), davidson=(10, 10, 1e-10), rdm=True, full=True,
+                     carryover=(0.3, 1e-3, 1e-4)),
+    "syn12_co": dict(synthetic=(12, 5, 5, 200, 150, 31), davidson=(10, 10, 1e-10), rdm=False, full=True,
+                     carryover=(0.25, 1e-4, 1e-5)),
     "fci12": dict(synthetic_named="fci12", davidson=(10, 10, 1e-8), rdm=False, full=False),
 }
 
@@ -76,6 +81,8 @@ def run_case(name: str, spec: dict, out_dir: str):
         cmd += ["--davidson", str(it), str(nb), repr(tol)]
         if spec["rdm"]:
             cmd += ["--rdm"]
+        if "carryover" in spec:
+            cmd += ["--carryover"] + [repr(v) for v in spec["carryover"]]
         env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
         subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
         L = synth.read_fcidump(fd)[0]
@@ -112,6 +119,16 @@ def run_case(name: str, spec: dict, out_dir: str):
             data["rdm2_idx"] = ridx
             data["rdm2_sample"] = r2[ridx]
             data["rdm2_sum"] = np.array([r2.sum(), (r2 * r2).sum(), np.abs(r2).sum()])
+        if "carryover" in spec:
+            # carry-over strings of W: co1 (threshold), co1r (ratio), co2 (co1 + singles; equal
+            # electron counts only), co3 (singles of determinants above the cutoff)
+            for tag in ("co1", "co1r", "co2", "co3"):
+                for s_ in ("a", "b"):
+                    f = os.path.join(tmp, f"{tag}_{s_}.u64")
+                    if os.path.exists(f):
+                        data[f"{tag}_{s_}"] = np.fromfile(f, dtype=np.uint64)
+            vals = [float(x) for x in open(os.path.join(tmp, "carryover.txt")).read().split()]
+            data["carryover"] = np.array(vals)  # ratio, threshold, cutoff, truncated a/b, total
         # the integrals as the reference's SetupIntegrals holds them (h1, packed store, core)
         _, _, h1, eri, core = synth.read_fcidump(fd)
         data["h1"], data["eri"], data["core"] = h1, eri, np.array([core])
@@ -128,6 +145,8 @@ def run_case(name: str, spec: dict, out_dir: str):
             meta["synthetic"] = list(spec["synthetic"])
         if "synthetic_named" in spec:
             meta["synthetic_named"] = spec["synthetic_named"]
+        if "carryover" in spec:
+            meta["carryover"] = list(spec["carryover"])
         return meta
 
 
