@@ -281,8 +281,9 @@ def carryover_measure(h, prob, cpu_sample=True):
     W = torch.randn(N, dtype=torch.float64, device=f"cuda:{h.device}", generator=g)
     W /= torch.linalg.vector_norm(W)
     out = {}
+    # cutoff at half the mean weight 1/N: about half the determinants of a random vector pass it
     for name, kind, thr in (("dominant", sbd_tpb.CARRYOVER_DOMINANT, 0.01),
-                            ("cutoff_singles", sbd_tpb.CARRYOVER_CUTOFF_SINGLES, 1e-7)):
+                            ("cutoff_singles", sbd_tpb.CARRYOVER_CUTOFF_SINGLES, 0.5 / N)):
         for _ in range(3):
             r = h.carryover(W, kind, 0.0, thr, mem=sbd_tpb.DEVICE)
         ts = []

@@ -163,28 +163,61 @@ __global__ void __launch_bounds__(kCoThreads) string_weights_kernel(const double
   }
 }
 
-// column j: sum of the nbands CTA partials, in band order; block 0 thread 0 also adds the totals
+// column j: sum of the nbands CTA partials.  A CTA covers 32 columns with 8 band groups; thread
+// (g, j) adds bands g, g+8, ... into four accumulators (four independent loads in flight), the
+// groups are then added in group order, so the result is the same on every run.  Block 0 also
+// adds the per-CTA totals the same way.
 template <bool COUNT>
-__global__ void column_reduce_kernel(size_t nb, int nbands, const double *__restrict__ colw,
-                                     const uint32_t *__restrict__ colc, const double *__restrict__ tot,
-                                     double *__restrict__ wb, uint32_t *__restrict__ cb,
-                                     double *__restrict__ total) {
-  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) column_reduce_kernel(size_t nb, int nbands, const double *__restrict__ colw,
+                                                            const uint32_t *__restrict__ colc,
+                                                            const double *__restrict__ tot, double *__restrict__ wb,
+                                                            uint32_t *__restrict__ cb, double *__restrict__ total) {
+  __shared__ double sv[8][33];
+  __shared__ uint32_t sn[8][33];
+  const int cx = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const size_t j = (size_t)blockIdx.x * 32 + cx;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  uint32_t c[4] = {0u, 0u, 0u, 0u};
   if (j < nb) {
-    if (COUNT) {
-      uint32_t c = 0;
-      for (int b = 0; b < nbands; b++) c += colc[(size_t)b * nb + j];
-      cb[j] = c;
-    } else {
-      double s = 0.0;
-      for (int b = 0; b < nbands; b++) s += colw[(size_t)b * nb + j];
-      wb[j] = s;
+    int b = g;
+    for (; b + 24 < nbands; b += 32) {
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (COUNT) c[u] += colc[(size_t)(b + 8 * u) * nb + j];
+        else s[u] += colw[(size_t)(b + 8 * u) * nb + j];
+      }
+    }
+    for (; b < nbands; b += 8) {
+      if (COUNT) c[0] += colc[(size_t)b * nb + j];
+      else s[0] += colw[(size_t)b * nb + j];
     }
   }
-  if (COUNT && blockIdx.x == 0 && threadIdx.x == 0) {
+  sv[g][cx] = (s[0] + s[1]) + (s[2] + s[3]);
+  sn[g][cx] = (c[0] + c[1]) + (c[2] + c[3]);
+  __syncthreads();
+  if (g == 0 && j < nb) {
+    if (COUNT) {
+      uint32_t t = 0;
+      for (int k = 0; k < 8; k++) t += sn[k][cx];
+      cb[j] = t;
+    } else {
+      double t = 0.0;
+      for (int k = 0; k < 8; k++) t += sv[k][cx];
+      wb[j] = t;
+    }
+  }
+  if (COUNT && blockIdx.x == 0) {
+    __syncthreads();
     double t = 0.0;
-    for (int b = 0; b < nbands; b++) t += tot[b];
-    *total = t;
+    for (int b = threadIdx.x; b < nbands; b += 256) t += tot[b];
+    sv[g][cx] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0;
+      for (int k = 0; k < 8; k++)
+        for (int x = 0; x < 32; x++) a += sv[k][x];
+      *total = a;
+    }
   }
 }
 
@@ -268,24 +301,22 @@ __global__ void singles_extend_kernel(const uint64_t *__restrict__ s, size_t n, 
 
 inline unsigned grid_for(size_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-// device buffers freed on scope exit
+// device buffers from the handle's pool, returned to it on scope exit (repeated calls of the same
+// size allocate nothing)
 struct Scratch {
-  std::vector<void *> ptrs;
+  sbd_tpb_handle *h;
+  std::vector<std::pair<void *, size_t>> got;
+  explicit Scratch(sbd_tpb_handle *hh) : h(hh) {}
   ~Scratch() {
-    for (void *p : ptrs) cudaFree(p);
+    for (auto &g : got) pool_put(h, g.first, g.second);
   }
   template <typename T>
   int get(T **out, size_t count) {
     *out = nullptr;
-    if (count == 0) count = 1;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(e == cudaErrorMemoryAllocation ? SBD_TPB_ERR_OOM : SBD_TPB_ERR_CUDA,
-                  std::string("carry-over scratch: ") + cudaGetErrorString(e));
-    }
-    ptrs.push_back(p);
+    TPB_CHECK(pool_get(h, bytes, &p));
+    got.emplace_back(p, bytes);
     *out = (T *)p;
     return SBD_TPB_OK;
   }
@@ -296,7 +327,8 @@ template <bool COUNT>
 int string_weights(sbd_tpb_handle *h, const double *dW, double cutoff, Scratch &sc, double *wa, double *wb,
                    uint32_t *ca, uint32_t *cb, double *total) {
   const size_t na = h->astr.size(), nb = h->bstr.size();
-  const int nbands = (int)std::max<size_t>(1, std::min<size_t>(na, (size_t)h->num_sms * 4));
+  // six CTAs of 256 threads fit an SM (40 registers a thread): one full wave
+  const int nbands = (int)std::max<size_t>(1, std::min<size_t>(na, (size_t)h->num_sms * 6));
   double *colw = nullptr, *tot = nullptr;
   uint32_t *colc = nullptr;
   if (COUNT) {
@@ -305,12 +337,15 @@ int string_weights(sbd_tpb_handle *h, const double *dW, double cutoff, Scratch &
   } else {
     TPB_CHECK(sc.get(&colw, (size_t)nbands * nb));
   }
+  // timed from here: the scratch above is allocated before the first event
+  TPB_CUDA(cudaEventRecord(h->ev_co[0], h->stream));
   string_weights_kernel<COUNT><<<nbands, kCoThreads, 0, h->stream>>>(dW, na, nb, nbands, cutoff, wa, ca, colw,
                                                                       colc, tot);
   TPB_LAUNCHED(h);
-  column_reduce_kernel<COUNT><<<grid_for(nb, 256), 256, 0, h->stream>>>(nb, nbands, colw, colc, tot, wb, cb,
-                                                                         total);
+  column_reduce_kernel<COUNT><<<grid_for(nb, 32), 256, 0, h->stream>>>(nb, nbands, colw, colc, tot, wb, cb,
+                                                                        total);
   TPB_LAUNCHED(h);
+  TPB_CUDA(cudaEventRecord(h->ev_co[1], h->stream));
   return SBD_TPB_OK;
 }
 
@@ -432,7 +467,7 @@ int carryover_device(sbd_tpb_handle *h, const double *dW, sbd_tpb_carryover *co)
   if (na > (size_t)INT32_MAX || nb > (size_t)INT32_MAX)
     return fail(SBD_TPB_ERR_INVALID, "carry-over: more than 2^31 strings of one spin");
   const auto t0 = std::chrono::steady_clock::now();
-  Scratch sc;
+  Scratch sc(h);
   co->truncated_a = co->truncated_b = 0.0;
   co->total_weight = 0.0;
   uint64_t *ra = nullptr, *rb = nullptr;
@@ -441,9 +476,7 @@ int carryover_device(sbd_tpb_handle *h, const double *dW, sbd_tpb_carryover *co)
     double *wa = nullptr, *wb = nullptr;
     TPB_CHECK(sc.get(&wa, na));
     TPB_CHECK(sc.get(&wb, nb));
-    TPB_CUDA(cudaEventRecord(h->ev_co[0], h->stream));
     TPB_CHECK(string_weights<false>(h, dW, 0.0, sc, wa, wb, nullptr, nullptr, nullptr));
-    TPB_CUDA(cudaEventRecord(h->ev_co[1], h->stream));
     TPB_CHECK(select_dominant(h, wa, h->d_astr, na, co->ratio, co->threshold, sc, &ra, &nra, &co->truncated_a));
     TPB_CHECK(select_dominant(h, wb, h->d_bstr, nb, co->ratio, co->threshold, sc, &rb, &nrb, &co->truncated_b));
   } else {
@@ -452,9 +485,7 @@ int carryover_device(sbd_tpb_handle *h, const double *dW, sbd_tpb_carryover *co)
     TPB_CHECK(sc.get(&ca, na));
     TPB_CHECK(sc.get(&cb, nb));
     TPB_CHECK(sc.get(&tot, 1));
-    TPB_CUDA(cudaEventRecord(h->ev_co[0], h->stream));
     TPB_CHECK(string_weights<true>(h, dW, co->threshold, sc, nullptr, nullptr, ca, cb, tot));
-    TPB_CUDA(cudaEventRecord(h->ev_co[1], h->stream));
     TPB_CUDA(cudaMemcpyAsync(&co->total_weight, tot, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     TPB_CHECK(select_counted(h, ca, h->d_astr, na, sc, &ra, &nra));
     TPB_CHECK(select_counted(h, cb, h->d_bstr, nb, sc, &rb, &nrb));
