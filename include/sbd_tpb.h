@@ -53,6 +53,10 @@ extern "C" {
                            alpha-beta contraction, FP64 dots / Rayleigh-Ritz and a final FP64
                            sigma for the reported energy and residual */
 
+/* Eigensolver (--method of the reference app; the matrix-free ones). */
+#define SBD_TPB_METHOD_DAVIDSON 0 /* block Davidson (tpb/davidson.h:667-930) */
+#define SBD_TPB_METHOD_LANCZOS 2  /* Lanczos without reorthogonalisation (tpb/lanczos.h:167-320), FP64 */
+
 /* Davidson correction. */
 #define SBD_TPB_PRECOND_DIAGONAL 0 /* t = r / (E0 - H_ii)  (tpb/davidson.h:858-868) */
 #define SBD_TPB_PRECOND_LEARNED 1  /* MLP correction, diagonal fallback when a step fails */
@@ -76,6 +80,7 @@ typedef struct sbd_tpb_params {
                         the alpha<->beta exchange-symmetric sector the start vector lies in
                         (C = C^T in the separated convention), so rounding cannot steer the
                         iteration to a lower state of the other sector; 0: off */
+  int method;        /* --method: SBD_TPB_METHOD_DAVIDSON (default) or SBD_TPB_METHOD_LANCZOS */
 } sbd_tpb_params;
 
 /* Fills p with the reference defaults (tpb/sbdiag.h:22-50) and SBD_TPB_FP64 / diagonal. */
@@ -216,6 +221,14 @@ SBD_TPB_API int sbd_tpb_sigma_noalloc(sbd_tpb_handle *h, const void *C, void *si
  * result (ci_vector/density/RDM fields as in sbd_tpb_diag). */
 SBD_TPB_API int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params, const double *W0,
                      sbd_tpb_result *result);
+
+/* Lanczos (tpb/lanczos.h:167-320; --method 2) on the handle's problem from W0 (as
+ * sbd_tpb_davidson): params->max_it outer iterations of at most params->max_nb steps, stopping
+ * when the lowest eigenvalue of the tridiagonal matrix moves by less than params->eps (result
+ * converged = 1) or an off-diagonal falls below it; params->verbose prints the reference's
+ * " Lanczos iteration" lines.  FP64 only.  result->residual is |HW - E W| of the final vector. */
+SBD_TPB_API int sbd_tpb_lanczos(sbd_tpb_handle *h, const sbd_tpb_params *params, const double *W0,
+                                sbd_tpb_result *result);
 
 /* 1/2-RDMs of W; replaces Correlation (tpb/correlation.h:378-664) and
  * MultTPBThrust::correlation (tpb/correlation_thrust.h:504-731).  one: [2*L*L], two: [4*L^4]

@@ -79,6 +79,10 @@ def lib():
         L.orc_reorder_sign.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                       _f32p, _f32p, _f32p, _f32p]
+        L.orc_lanczos.restype = C.c_int
+        L.orc_lanczos.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.POINTER(Tables), C.POINTER(Ham),
+                                  _f64p, _f64p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_string_weights.argtypes = [_f64p, C.c_size_t, C.c_size_t, C.c_double, _f64p, _f64p, _u64p, _u64p,
                                          C.POINTER(C.c_double)]
         L.orc_carryover_select.restype = C.c_size_t
@@ -211,6 +215,21 @@ class System:
         ns = lib().orc_davidson(self.astr, self.na, self.bstr, self.nb, C.byref(self.t), C.byref(self.ham.h),
                                 hii, W, max_it, max_nb, eps, int(verbose), C.byref(e), C.byref(r))
         return e.value, W, ns, r.value
+
+    def lanczos(self, max_it=10, num_block=10, eps=1e-8, verbose=False, W0=None):
+        """(energy, W, sigma applications, printed lines, converged) of orc_lanczos from the first
+        determinant (or W0)."""
+        hii = self.diagonal()
+        W = np.zeros(self.na * self.nb)
+        if W0 is None:
+            W[0] = 1.0
+        else:
+            W[:] = W0
+        e, printed, conv = C.c_double(0), C.c_int(0), C.c_int(0)
+        ns = lib().orc_lanczos(self.astr, self.na, self.bstr, self.nb, C.byref(self.t), C.byref(self.ham.h),
+                               hii, W, max_it, num_block, eps, int(verbose), C.byref(e), C.byref(printed),
+                               C.byref(conv))
+        return e.value, W, ns, printed.value, bool(conv.value)
 
     def rdm(self, W: np.ndarray):
         L = self.ham.L

@@ -14,6 +14,8 @@
 //   davidson.txt / W.f64  Davidson (tpb/davidson.h:667-930) from the HF start, energy as in
 //                         tpb/sbdiag.h:431-469
 //   rdm1.f64 / rdm2.f64   Correlation (tpb/correlation.h:378-664)
+//   lanczos.txt / W_lanczos.f64   Lanczos (tpb/lanczos.h:167-320) from the HF start: energy
+//                         <W|H|W> (as tpb/sbdiag.h:431-469) and the final vector
 //   co<k>_{a,b}.u64, carryover.txt   carry-over strings of W (tpb/sbdiag.h:690-736):
 //                         co1 = CarryOverAdet/Bdet with the threshold (tpb/rdmat.h:63-100,
 //                         190-227), co1r = the same with n_kept = ratio * size (:102-135,
@@ -27,6 +29,7 @@
 //
 // Usage: ref_dump --fcidump F --adetfile A [--bdetfile B] [--bit_length 20] --out DIR
 //                 [--sigma_seed S] [--davidson IT NB TOL] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
+//                 [--lanczos IT NB TOL]
 // The reference headers rely on their includer for these (as its app main.cc does).
 #include <chrono>
 #include <cmath>
@@ -93,6 +96,8 @@ int main(int argc, char **argv) {
   double dav_tol = 1e-8;
   bool do_rdm = false;
   double co_ratio = -1.0, co_threshold = 0.0, co_cutoff = 0.0;
+  int lz_it = 0, lz_nb = 0;
+  double lz_tol = 1e-8;
   for (int i = 1; i < argc; ++i) {
     std::string a(argv[i]);
     if (a == "--fcidump") fcidumpfile = argv[++i];
@@ -106,7 +111,11 @@ int main(int argc, char **argv) {
       dav_nb = std::atoi(argv[++i]);
       dav_tol = std::atof(argv[++i]);
     } else if (a == "--rdm") do_rdm = true;
-    else if (a == "--carryover") {
+    else if (a == "--lanczos") {
+      lz_it = std::atoi(argv[++i]);
+      lz_nb = std::atoi(argv[++i]);
+      lz_tol = std::atof(argv[++i]);
+    } else if (a == "--carryover") {
       co_ratio = std::atof(argv[++i]);
       co_threshold = std::atof(argv[++i]);
       co_cutoff = std::atof(argv[++i]);
@@ -245,6 +254,21 @@ int main(int argc, char **argv) {
       oc.precision(17);
       oc << co_ratio << " " << co_threshold << " " << co_cutoff << " " << tw_a << " " << tw_b << " " << total << "\n";
     }
+  }
+  if (lz_it > 0) {
+    std::vector<double> W;
+    sbd::BasisInitVector(W, adet, bdet, 1, 1, h_comm, b_comm, t_comm, 0, 1729);
+    sbd::Lanczos(hii, W, adet, bdet, bit_length, static_cast<size_t>(L), 1, 1, helper, I0, I1, I2,
+                 h_comm, b_comm, t_comm, lz_it, lz_nb, lz_tol);
+    std::vector<double> C(W.size(), 0.0);
+    sbd::mult(hii, W, C, adet, bdet, bit_length, static_cast<size_t>(L), 1, 1, helper, I0, I1, I2,
+              h_comm, b_comm, t_comm);
+    double E = 0.0;
+    sbd::InnerProduct(W, C, E, b_comm);
+    std::ofstream ofs(out + "/lanczos.txt");
+    ofs.precision(17);
+    ofs << E << "\n";
+    write_raw(out + "/W_lanczos.f64", W.data(), W.size());
   }
   MPI_Finalize();
   return 0;

@@ -678,6 +678,88 @@ int orc_davidson(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t n
   return nsigma;
 }
 
+int orc_lanczos(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                const orc_tables *t, const orc_ham *h, const double *hii, double *W,
+                int max_it, int num_block, double eps, int verbose, double *energy, int *steps_printed,
+                int *converged) {
+  const size_t n = na * nb;
+  const int lda = num_block;
+  double *A = calloc((size_t)lda * lda, sizeof(double));
+  double *U = calloc((size_t)lda * lda, sizeof(double));
+  double *E = calloc((size_t)lda, sizeof(double));
+  double *HC = malloc(n * sizeof(double));
+  double **C = malloc((size_t)lda * sizeof(double *));
+  for (int b = 0; b < lda; b++) C[b] = malloc(n * sizeof(double));
+  int nsigma = 0, printed = 0, stop_it = 0;
+  for (int it = 0; it < max_it; it++) {
+    /* C[0] = W; HC = 0 (tpb/lanczos.h:204-214) */
+    memcpy(C[0], W, n * sizeof(double));
+    memset(HC, 0, n * sizeof(double));
+    int m = 0;
+    double E_old = 1.0e+8;
+    stop_it = 0;
+    for (int ib = 0; ib < num_block; ib++) {
+      m++;
+      /* HC += H C[ib]; A[ib][ib] = <C[ib], HC> (:216-226) */
+      orc_sigma(astr, na, bstr, nb, t, h, hii, C[ib], HC);
+      nsigma++;
+      A[ib + lda * ib] = kahan_dot(C[ib], HC, n);
+      for (int i = 0; i < m; i++)
+        for (int j = 0; j < m; j++) U[i + lda * j] = A[i + lda * j];
+      jacobi_sorted(m, U, lda, E);
+      /* stop on a small eigenvalue change, or at the last block (:234-241) */
+      if (fabs(E[0] - E_old) < eps) {
+        stop_it = 1;
+        break;
+      }
+      E_old = E[0];
+      if (ib + 1 == num_block) break;
+      /* C[ib+1] = normalised (HC - a C[ib]), b = its norm (:243-254) */
+      const double a = A[ib + lda * ib];
+#pragma omp parallel for schedule(static)
+      for (size_t s = 0; s < n; s++) HC[s] -= a * C[ib][s];
+      memcpy(C[ib + 1], HC, n * sizeof(double));
+      const double b = normalize(C[ib + 1], n);
+      A[ib + lda * (ib + 1)] = b;
+      A[ib + 1 + lda * ib] = b;
+      printed++;
+      if (verbose) {
+        printf(" Lanczos iteration %d, step %d: (A,B)=(%.16g,%.16g):", it, ib, a, b);
+        for (int q = 0; q < (m < 4 ? m : 4); q++) printf(" %.16g", E[q]);
+        printf("\n");
+      }
+      if (fabs(b) < eps) break;
+      /* HC = -b C[ib] (:275-285, one rank) */
+#pragma omp parallel for schedule(static)
+      for (size_t s = 0; s < n; s++) HC[s] = -b * C[ib][s];
+    }
+    /* W = sum_k U[k][0] C[k] (:288-305) */
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < m; j++) U[i + lda * j] = A[i + lda * j];
+    jacobi_sorted(m, U, lda, E);
+#pragma omp parallel for schedule(static)
+    for (size_t s = 0; s < n; s++) {
+      double w = U[0] * C[0][s];
+      for (int k = 1; k < m; k++) w += U[k] * C[k][s];
+      W[s] = w;
+    }
+    if (stop_it) break;
+  }
+  double *Cw = calloc(n, sizeof(double));
+  orc_sigma(astr, na, bstr, nb, t, h, hii, W, Cw);
+  *energy = kahan_dot(W, Cw, n);
+  if (steps_printed) *steps_printed = printed;
+  if (converged) *converged = stop_it;
+  free(Cw);
+  for (int b = 0; b < lda; b++) free(C[b]);
+  free(C);
+  free(HC);
+  free(A);
+  free(U);
+  free(E);
+  return nsigma;
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* RDMs (tpb/correlation.h:378-664, basic/correlation.h:16-231)                                */
 /* ------------------------------------------------------------------------------------------ */

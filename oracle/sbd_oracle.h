@@ -100,6 +100,16 @@ int orc_davidson(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t n
                  const orc_tables *t, const orc_ham *h, const double *hii, double *W,
                  int max_it, int max_nb, double eps, int verbose, double *energy, double *resid);
 
+/* Lanczos for the lowest root without reorthogonalisation (tpb/lanczos.h:167-320), from W
+ * (in/out, not renormalised), with the dense subspace eigenproblem solved by the same sorted
+ * Jacobi method as orc_davidson.  Returns the number of sigma applications; *energy is <W|H|W>
+ * after the loop (tpb/sbdiag.h:431-469), *steps_printed the number of " Lanczos iteration"
+ * lines the reference prints, *converged whether the eigenvalue change fell below eps. */
+int orc_lanczos(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                const orc_tables *t, const orc_ham *h, const double *hii, double *W,
+                int max_it, int num_block, double eps, int verbose, double *energy, int *steps_printed,
+                int *converged);
+
 /* Spin-resolved RDMs of W (tpb/correlation.h:378-664, basic/correlation.h:16-231):
  * one[s*L*L + i + L*j], two[(s+2t)*L^4 + ...] in the reference layout. */
 void orc_rdm(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,

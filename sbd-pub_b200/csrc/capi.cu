@@ -85,6 +85,7 @@ void sbd_tpb_default_params(sbd_tpb_params *p) {
   p->verbose = 0;
   p->device = 0;
   p->symmetry = 1;
+  p->method = SBD_TPB_METHOD_DAVIDSON;
 }
 
 const char *sbd_tpb_last_error(void) { return g_last_error.c_str(); }
@@ -343,6 +344,14 @@ int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params, const doub
   return davidson_run(h, params, W0, result);
 }
 
+int sbd_tpb_lanczos(sbd_tpb_handle *h, const sbd_tpb_params *params, const double *W0,
+                    sbd_tpb_result *result) {
+  TPB_HANDLE(h);
+  if (!params || !result) return fail(SBD_TPB_ERR_INVALID, "null params/result");
+  if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
+  return lanczos_run(h, params, W0, result);
+}
+
 int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, int mem) {
   TPB_HANDLE(h);
   if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
@@ -415,7 +424,9 @@ int sbd_tpb_diag_from(const sbd_tpb_params *params, const sbd_tpb_hamiltonian *h
       result->one_rdm = nullptr;
       result->two_rdm = nullptr;
     }
-    rc = sbd_tpb_davidson(h, params, W0, result);
+    if (params->method == SBD_TPB_METHOD_LANCZOS) rc = sbd_tpb_lanczos(h, params, W0, result);
+    else if (params->method == SBD_TPB_METHOD_DAVIDSON) rc = sbd_tpb_davidson(h, params, W0, result);
+    else rc = fail(SBD_TPB_ERR_INVALID, "method must be 0 (Davidson) or 2 (Lanczos)");
     result->one_rdm = one;
     result->two_rdm = two;
   }

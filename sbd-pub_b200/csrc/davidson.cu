@@ -89,24 +89,6 @@ void jacobi_eigen(int n, const double *A, int lda, std::vector<double> &E, std::
 }
 
 template <typename T>
-struct DevVec {
-  sbd_tpb_handle *h = nullptr;
-  T *p = nullptr;
-  size_t bytes = 0;
-  int get(sbd_tpb_handle *hh, size_t count) {
-    h = hh;
-    bytes = count * sizeof(T);
-    void *q = nullptr;
-    const int rc = pool_get(h, bytes, &q);
-    p = static_cast<T *>(q);
-    return rc;
-  }
-  ~DevVec() {
-    if (p) pool_put(h, p, bytes);
-  }
-};
-
-template <typename T>
 int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, double shift,
               double *dWout, double *resid_out, int *nsigma_out, int *converged_out, DavRecord *rec,
               sbd_tpb_precond *learned, double *energy_out, int *learned_steps, int *fallback_steps) {
@@ -409,7 +391,7 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
     return fail(SBD_TPB_ERR_INVALID, "davidson: unknown preconditioner");
   }
   int nl = 0, nf = 0;
-  DevVec<double> dW, dHW;
+  DevVec<double> dW;
   TPB_CHECK(dW.get(h, n));
   if (p->precision == SBD_TPB_MIXED) {
     double h00 = 0.0;
@@ -420,34 +402,41 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   }
   res->learned_steps = nl;
   res->fallback_steps = nf;
+  return solve_finish(h, dW.p, res, t0, nsig, conv, p->precision == SBD_TPB_MIXED ? -1.0 : resid);
+}
+
+int solve_finish(sbd_tpb_handle *h, double *dW, sbd_tpb_result *res,
+                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid) {
+  const size_t n = h->ndet();
   // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
+  DevVec<double> dHW;
   TPB_CHECK(dHW.get(h, n));
   double E = 0.0, rr = 0.0;
-  TPB_CHECK(sigma_sep<double>(h, dW.p, dHW.p, 0));
-  const double *wp[1] = {dW.p};
+  TPB_CHECK(sigma_sep<double>(h, dW, dHW.p, 0));
+  const double *wp[1] = {dW};
   TPB_CHECK(multi_dot<double>(h, wp, 1, dHW.p, n, &E));
-  TPB_CHECK(axpby<double>(h, dW.p, dHW.p, -E, 1.0, n));
+  TPB_CHECK(axpby<double>(h, dW, dHW.p, -E, 1.0, n));
   const double *hp[1] = {dHW.p};
   TPB_CHECK(multi_dot<double>(h, hp, 1, dHW.p, n, &rr));
   if (res->ci_vector) {
-    TPB_CHECK(reorder_sign_apply_f64(h, dW.p, dHW.p));
+    TPB_CHECK(reorder_sign_apply_f64(h, dW, dHW.p));
     TPB_CUDA(cudaMemcpyAsync(res->ci_vector, dHW.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
                              h->stream));
   }
   TPB_CUDA(cudaStreamSynchronize(h->stream));
   if (res->density || res->one_rdm || res->two_rdm) {
     if (res->one_rdm || res->two_rdm) pool_clear(h);  // the 2-RDM passes need their own N-vectors
-    TPB_CHECK(rdm_sep(h, dW.p, res->one_rdm, res->two_rdm, res->density));
+    TPB_CHECK(rdm_sep(h, dW, res->one_rdm, res->two_rdm, res->density));
   }
   // carry-over strings of the final vector (tpb/sbdiag.h:690-736); a short caller buffer is
   // reported after the rest of the result is filled
   int co_rc = SBD_TPB_OK;
   if (res->carryover && res->carryover->type != SBD_TPB_CARRYOVER_NONE) {
-    co_rc = carryover_device(h, dW.p, res->carryover);
+    co_rc = carryover_device(h, dW, res->carryover);
     if (co_rc != SBD_TPB_OK && co_rc != SBD_TPB_ERR_CAPACITY) return co_rc;
   }
   res->energy = E;
-  res->residual = (p->precision == SBD_TPB_MIXED) ? std::sqrt(rr) : resid;
+  res->residual = resid < 0.0 ? std::sqrt(rr) : resid;
   res->iterations = nsig;
   res->converged = conv;
   res->seconds_davidson = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
+
 #include <string>
 #include <vector>
 
@@ -223,8 +225,39 @@ int multi_dot(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n,
 int pool_get(sbd_tpb_handle *h, size_t bytes, void **out);
 void pool_put(sbd_tpb_handle *h, void *p, size_t bytes);
 void pool_clear(sbd_tpb_handle *h);
+// an N-vector from the pool, returned to it on scope exit (or by release())
+template <typename T>
+struct DevVec {
+  sbd_tpb_handle *h = nullptr;
+  T *p = nullptr;
+  size_t bytes = 0;
+  int get(sbd_tpb_handle *hh, size_t count) {
+    h = hh;
+    bytes = count * sizeof(T);
+    void *q = nullptr;
+    const int rc = pool_get(h, bytes, &q);
+    p = static_cast<T *>(q);
+    return rc;
+  }
+  DevVec() = default;
+  DevVec(const DevVec &) = delete;
+  DevVec &operator=(const DevVec &) = delete;
+  DevVec(DevVec &&o) noexcept : h(o.h), p(o.p), bytes(o.bytes) { o.p = nullptr; }
+  void release() {
+    if (p) pool_put(h, p, bytes);
+    p = nullptr;
+  }
+  ~DevVec() { release(); }
+};
 int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double *density);
 // davidson.cu
 int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
                  sbd_tpb_result *res);
+// after a solve: final FP64 sigma of the device vector dW (separated convention) for the energy
+// <W|H|W> and |HW - E W| (reported unless resid >= 0 is given), then the caller's CI vector,
+// occupations/RDMs and carry-over strings; fills res and returns the solve's status
+int solve_finish(sbd_tpb_handle *h, double *dW, sbd_tpb_result *res,
+                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid);
+// lanczos.cu
+int lanczos_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0, sbd_tpb_result *res);
 }  // namespace sbdtpb

@@ -11,6 +11,8 @@
 // the carry-over strings on the GPU (tpb/sbdiag.h:690-736) and --carryover_adetfile /
 // --carryover_bdetfile write them (main.cc:203-224).  Flags for parts outside this build
 // (--dump_matrix_form_wf, more than one rank per communicator) are reported and rejected.
+// --method 0 runs Davidson, --method 2 Lanczos (tpb/lanczos.h:167-320, its " Lanczos iteration"
+// lines); the stored-Hamiltonian methods 1 and 3 are not built.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -100,7 +102,8 @@ int main(int argc, char **argv) {
              a == "--thrust_collapse_loops") next();
   }
   if (bit_length == 0 || bit_length > 64) die("--bit_length must be in [1, 64]");
-  if (method != 0) die("only --method 0 (matrix-free Davidson) is built");
+  if (method != 0 && method != 2) die("only the matrix-free solvers are built: --method 0 (Davidson) or 2 (Lanczos)");
+  prm.method = method;
   if (comm_sizes != 1) die("one rank on one GPU: --*_comm_size must be 1");
   if (prm.init != 0) die("only --init 0 (start from the first determinant) is built");
   if (carryover_type < 0 || carryover_type > 3) die("--carryover_type must be 0, 1, 2 or 3");
@@ -180,7 +183,8 @@ int main(int argc, char **argv) {
       die(sbd_tpb_last_error());
     res.seconds_tables = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
     if (!prm.do_rdm) res.one_rdm = res.two_rdm = nullptr;
-    rc = sbd_tpb_davidson(h, &prm, W0.empty() ? nullptr : W0.data(), &res);
+    rc = method == 2 ? sbd_tpb_lanczos(h, &prm, W0.empty() ? nullptr : W0.data(), &res)
+                     : sbd_tpb_davidson(h, &prm, W0.empty() ? nullptr : W0.data(), &res);
     const std::string msg = rc == SBD_TPB_OK ? std::string() : std::string(sbd_tpb_last_error());
     sbd_tpb_destroy(h);
     sbd_tpb_precond_destroy(pc);

@@ -30,6 +30,7 @@ ERR_NO_DEVICE = -7
 HOST, DEVICE = 0, 1
 SINGLES_ALPHA, DOUBLES_ALPHA, SINGLES_BETA, DOUBLES_BETA = 0, 1, 2, 3
 FP64, MIXED = 0, 1
+METHOD_DAVIDSON, METHOD_LANCZOS = 0, 2
 PRECOND_DIAGONAL, PRECOND_LEARNED = 0, 1
 
 # Every function the header declares (the symbol test checks the library against this list).
@@ -43,7 +44,7 @@ EXPORTED = [
     "sbd_tpb_precond_num_samples", "sbd_tpb_precond_train", "sbd_tpb_precond_evaluate",
     "sbd_tpb_precond_get_params", "sbd_tpb_precond_set_params", "sbd_tpb_precond_gradients",
     "sbd_tpb_precond_apply", "sbd_tpb_set_preconditioner", "sbd_tpb_carryover_strings",
-    "sbd_tpb_carryover_capacity", "sbd_tpb_last_carryover_ms",
+    "sbd_tpb_carryover_capacity", "sbd_tpb_last_carryover_ms", "sbd_tpb_lanczos",
 ]
 CARRYOVER_NONE, CARRYOVER_DOMINANT, CARRYOVER_DOMINANT_SINGLES, CARRYOVER_CUTOFF_SINGLES = 0, 1, 2, 3
 ERR_CAPACITY = -8
@@ -60,7 +61,7 @@ class Params(C.Structure):
     _fields_ = [
         ("max_it", C.c_int), ("max_nb", C.c_int), ("eps", C.c_double), ("max_time", C.c_double),
         ("init", C.c_int), ("do_rdm", C.c_int), ("precision", C.c_int), ("preconditioner", C.c_int),
-        ("verbose", C.c_int), ("device", C.c_int), ("symmetry", C.c_int),
+        ("verbose", C.c_int), ("device", C.c_int), ("symmetry", C.c_int), ("method", C.c_int),
     ]
 
 
@@ -125,6 +126,7 @@ def lib():
     L.sbd_tpb_sigma_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.sbd_tpb_davidson.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
     L.sbd_tpb_rdm.argtypes = [vp, vp, vp, vp, C.c_int]
+    L.sbd_tpb_lanczos.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
     L.sbd_tpb_stream.restype = vp
     L.sbd_tpb_stream.argtypes = [vp]
     L.sbd_tpb_last_sigma_ms.restype = C.c_double
@@ -293,8 +295,9 @@ class Handle:
 
     def davidson(self, params: Params | None = None, W0: np.ndarray | None = None,
                  want_vector=True, want_rdm=False, carryover: tuple | None = None):
-        """Davidson on the handle's problem; carryover = (type, ratio, threshold) also returns the
-        carry-over strings of the final vector under "carryover"."""
+        """Davidson (or Lanczos when params.method == METHOD_LANCZOS) on the handle's problem;
+        carryover = (type, ratio, threshold) also returns the carry-over strings of the final vector
+        under "carryover"."""
         prob = self.problem
         params = params or default_params()
         res = Result()
@@ -312,8 +315,8 @@ class Handle:
             co, bufs = self._carryover_record(*carryover)
             res.carryover = C.pointer(co)
         w0 = None if W0 is None else np.ascontiguousarray(W0, np.float64)
-        rc = lib().sbd_tpb_davidson(self.h, C.byref(params), w0.ctypes.data if w0 is not None else None,
-                                    C.byref(res))
+        solver = lib().sbd_tpb_lanczos if params.method == METHOD_LANCZOS else lib().sbd_tpb_davidson
+        rc = solver(self.h, C.byref(params), w0.ctypes.data if w0 is not None else None, C.byref(res))
         _check(rc, allow=(OK, ERR_NOT_CONVERGED))
         return dict(energy=res.energy, residual=res.residual, iterations=res.iterations,
                     converged=bool(res.converged), W=W, density=dens, one=one, two=two,

@@ -43,18 +43,19 @@ def _synthetic_inputs(tmp, L, na_e, nb_e, na_cnt, nb_cnt, seed):
 CASES = {
     # name: (inputs, davidson (it, nb, tol), rdm, store_full)
     "n2_1em3": dict(fcidump=f"{REF}/data/n2/fcidump.txt", adet=f"{REF}/data/n2/1em3-alpha.txt",
-                    davidson=(10, 10, 1e-8), rdm=True, full=False,
+                    davidson=(10, 10, 1e-8), rdm=True, full=False, lanczos=(2, 40, 1e-8),
                     published=-109.04162110, published_src="data/n2/README.md:5"),
     "h2o_1em3": dict(fcidump=f"{REF}/data/h2o/fcidump.txt", adet=f"{REF}/data/h2o/h2o-1em3-alpha.txt",
                      davidson=(10, 10, 1e-8), rdm=False, full=False,
                      published=-76.23594663, published_src="data/h2o/README.md:6"),
-    # carryover = (ratio, threshold, cutoff) of the carry-over dumps (ref_dump --carryover)
+    # carryover = (ratio, threshold, cutoff) of the carry-over dumps (ref_dump --carryover);
+    # lanczos = (iterations, block, tolerance) of a Lanczos run (ref_dump --lanczos)
     "syn8": dict(synthetic=(8, 3, 3, 56, 56, 11), davidson=(10, 10, 1e-10), rdm=True, full=True,
-                 carryover=(0.5, 0.01, 1e-3)),
+                 carryover=(0.5, 0.01, 1e-3), lanczos=(3, 20, 1e-10)),
     "syn10_ab": dict(synthetic=(10, 4, 3, 120, 90, 23), davidson=(10, 10, 1e-10), rdm=True, full=True,
-                     carryover=(0.3, 1e-3, 1e-4)),
+                     carryover=(0.3, 1e-3, 1e-4), lanczos=(3, 20, 1e-10)),
     "syn12_co": dict(synthetic=(12, 5, 5, 200, 150, 31), davidson=(10, 10, 1e-10), rdm=False, full=True,
-                     carryover=(0.25, 1e-4, 1e-5)),
+                     carryover=(0.25, 1e-4, 1e-5), lanczos=(3, 30, 1e-10)),
     "fci12": dict(synthetic_named="fci12", davidson=(10, 10, 1e-8), rdm=False, full=False),
 }
 
@@ -83,8 +84,11 @@ def run_case(name: str, spec: dict, out_dir: str):
             cmd += ["--rdm"]
         if "carryover" in spec:
             cmd += ["--carryover"] + [repr(v) for v in spec["carryover"]]
+        if "lanczos" in spec:
+            cmd += ["--lanczos"] + [repr(v) for v in spec["lanczos"]]
         env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
-        subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+        out = subprocess.run(cmd, check=True, env=env, capture_output=True, text=True).stdout
+        lanczos_lines = sum(1 for l in out.splitlines() if l.startswith(" Lanczos iteration"))
         L = synth.read_fcidump(fd)[0]
         rd = lambda f, dt=np.float64: np.fromfile(os.path.join(tmp, f), dtype=dt)  # noqa: E731
         astr, bstr = rd("astr.u64", np.uint64), rd("bstr.u64", np.uint64)
@@ -129,6 +133,11 @@ def run_case(name: str, spec: dict, out_dir: str):
                         data[f"{tag}_{s_}"] = np.fromfile(f, dtype=np.uint64)
             vals = [float(x) for x in open(os.path.join(tmp, "carryover.txt")).read().split()]
             data["carryover"] = np.array(vals)  # ratio, threshold, cutoff, truncated a/b, total
+        if "lanczos" in spec:
+            # energy <W|H|W> after the reference's Lanczos and how many step lines it printed
+            data["lanczos"] = np.array([float(open(os.path.join(tmp, "lanczos.txt")).read()), lanczos_lines])
+            if spec["full"]:
+                data["W_lanczos"] = rd("W_lanczos.f64")
         # the integrals as the reference's SetupIntegrals holds them (h1, packed store, core)
         _, _, h1, eri, core = synth.read_fcidump(fd)
         data["h1"], data["eri"], data["core"] = h1, eri, np.array([core])
@@ -147,6 +156,8 @@ def run_case(name: str, spec: dict, out_dir: str):
             meta["synthetic_named"] = spec["synthetic_named"]
         if "carryover" in spec:
             meta["carryover"] = list(spec["carryover"])
+        if "lanczos" in spec:
+            meta["lanczos"] = list(spec["lanczos"])
         return meta
 
 
