@@ -10,7 +10,8 @@ path has no data exchange on one node in this build): every rank solves its own 
 `value` is the aggregate.  `--impl reference` times the reference's own CPU sigma (compiled
 unchanged under oracle/_ref) on a bounded sample of the same workload with all host threads.
 
-The line also carries `carryover`: the carry-over string selection (sbd_tpb_carryover_strings,
+The line also carries `strings` (a 2,000,000-line string file parsed, sorted and de-duplicated on
+the GPU, beside the reference's LoadAlphaDets on the host) and `carryover`: the carry-over string selection (sbd_tpb_carryover_strings,
 the step after the solve in the reference's sbd::tpb::diag) on an FP64 vector of the workload,
 with the roofline of its pass over W and the CPU restatement timed on a sample of rows.
 
@@ -316,6 +317,48 @@ def carryover_measure(h, prob, cpu_sample=True):
     return out
 
 
+def strings_measure(h, args, cpu_sample=True):
+    """String-file parsing (sbd_tpb_read_strings): a text file of 2,000,000 lines drawn with
+    repetition from the workload's strings (as a sampled-string file of the sample-based loop
+    holds them), parsed, sorted and de-duplicated on the GPU; beside it the reference's own
+    LoadAlphaDets on the same file, on the host cores (oracle/_ref/ref_bench --parse)."""
+    import synth
+    L, n, cnt = synth.CONFIGS[args.workload]
+    pool = synth.sample_strings(L, n, cnt)
+    rng = np.random.default_rng(5)
+    vals = np.asarray(pool, np.uint64)[rng.integers(0, len(pool), size=2_000_000)]
+    bits = ((vals[:, None] >> np.arange(L - 1, -1, -1, dtype=np.uint64)) & 1).astype(np.uint8) + ord("0")
+    text = np.concatenate([bits, np.full((len(vals), 1), ord("\n"), np.uint8)], axis=1).tobytes()
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "strings.txt")
+        with open(path, "wb") as f:
+            f.write(text)
+        for _ in range(2):
+            h.read_strings(path, L)
+        dev, wall = [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            got = h.read_strings(path, L)
+            wall.append(time.perf_counter() - t0)
+            dev.append(h.last_parse_ms())
+        out = {"lines": len(vals), "bytes": len(text), "unique": int(len(got)),
+               "device_ms": float(np.median(dev)), "call_ms": 1e3 * float(np.median(wall)),
+               "note": "device_ms: host-to-device copy of the file from pinned memory, newline index, "
+                       "parse, sort, unique (CUDA events); call_ms adds reading the file from disk"}
+        if cpu_sample and os.path.exists(REF_BENCH):
+            env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+            r = subprocess.run([REF_BENCH, "--parse", path, "--norb", str(L), "--reps", "2"], capture_output=True,
+                               text=True, env=env, check=True).stdout
+            kv = dict(tok.split("=", 1) for tok in r.split())
+            ts = [float(x) for x in kv["parse_s"].split(",")]
+            out["cpu_baseline"] = {"value_ms": 1e3 * min(ts), "cores": 1, "kind": "reference",
+                                   "sample": "the same file through the reference's LoadAlphaDets "
+                                             "(basic/makedeterminants.h:160-186, serial)",
+                                   "unique": int(kv["nstrings"])}
+    return out
+
+
 def time_to_solution(h, args):
     """Wall time of whole Davidson solves from the HF start: the FP64 reference answer (residual
     1e-6), then plain FP64, mixed precision and mixed precision + learned preconditioner, all to
@@ -447,6 +490,10 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.empty_cache()
         solve = time_to_solution(h, args)
 
+    strings = None
+    if not args.no_carryover and world == 1:
+        strings = strings_measure(h, args, cpu_sample=rank == 0 and not args.no_cpu)
+
     carry = None
     if not args.no_carryover and world == 1:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -474,7 +521,7 @@ def run_ours(args, world, rank, local, pg):
                        "l2": "inputs larger than L2 (vector of %.2f GB)" % (N * esz / 1e9),
                        "tables_s": t_tables, "setup_s": t1 - t0},
             "gpu_launches": launches, "clocks": clocks.summary(), "roofline": roofline, "e2e": e2e,
-            "cpu_baseline": cpu, "time_to_solution": solve, "carryover": carry,
+            "cpu_baseline": cpu, "time_to_solution": solve, "carryover": carry, "strings": strings,
         }
         print(json.dumps(line), flush=True)
     h.close()

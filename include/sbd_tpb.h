@@ -171,6 +171,27 @@ SBD_TPB_API int sbd_tpb_set_hamiltonian(sbd_tpb_handle *h, const sbd_tpb_hamilto
 SBD_TPB_API int sbd_tpb_set_strings(sbd_tpb_handle *h, const uint64_t *astr, size_t na, const uint64_t *bstr,
                         size_t nb);
 
+/* String files parsed, sorted and de-duplicated on the GPU, as LoadAlphaDets leaves them
+ * (basic/makedeterminants.h:160-186): text, one string per line with orbital 0 the last of the first
+ * norb characters (from_string, framework/bit_manipulation.h:215-230; trailing '\r'/spaces and
+ * empty lines are skipped, a short line or a character other than 0/1 is SBD_TPB_ERR_IO with the
+ * line number), or binary, ceil(norb/8)-byte big-endian records holding the string in their low
+ * norb bits (DecodeAlphaDets, makedeterminants.h:63-108).  The result is ascending and unique
+ * (sort_bitarray), ready for sbd_tpb_set_strings.  Strings go to out (host) when it holds them
+ * all; otherwise *count is set and SBD_TPB_ERR_CAPACITY returned (a text file has at most
+ * nbytes/(norb+1)+1 strings, a binary one nbytes/ceil(norb/8)). */
+#define SBD_TPB_STRINGS_TEXT 0
+#define SBD_TPB_STRINGS_BINARY 1
+SBD_TPB_API int sbd_tpb_parse_strings(sbd_tpb_handle *h, const void *bytes, size_t nbytes, int format, int norb,
+                                      uint64_t *out, size_t cap, size_t *count);
+/* The same from a file; the format follows the extension (".bin" binary, anything else text),
+ * as LoadAlphaDets decides it. */
+SBD_TPB_API int sbd_tpb_read_strings(sbd_tpb_handle *h, const char *path, int norb, uint64_t *out, size_t cap,
+                                     size_t *count);
+/* Device time (ms) of the last string parse on the handle: host-to-device copy, parse, sort and
+ * de-duplication (CUDA events on the handle's stream). */
+SBD_TPB_API double sbd_tpb_last_parse_ms(sbd_tpb_handle *h);
+
 /* Excitation tables on the GPU; replaces MakeHelpers/RemakeHelpers with GenerateExcitation
  * (tpb/helper.h:185-323, 710-854, 916-1226) for one rank. */
 SBD_TPB_API int sbd_tpb_build_tables(sbd_tpb_handle *h);

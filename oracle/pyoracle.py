@@ -52,6 +52,7 @@ def lib():
         L.orc_ham_from_arrays.argtypes = [C.c_int, C.c_int, C.c_double, _f64p, _f64p, C.POINTER(Ham)]
         L.orc_free_ham.argtypes = [C.POINTER(Ham)]
         L.orc_load_strings.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.orc_load_strings_bin.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
         L.orc_excitations.restype = C.c_size_t
         L.orc_excitations.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.c_int, C.c_int, C.c_int,
                                       _u64p, C.c_void_p, C.c_void_p]
@@ -149,6 +150,16 @@ def load_strings(path: str, L: int) -> np.ndarray:
     out = np.zeros(n.value, np.uint64)
     lib().orc_load_strings(path.encode(), L, out.ctypes.data, n.value, C.byref(n))
     return out
+
+
+def load_strings_bin(path: str, L: int) -> np.ndarray:
+    """Sorted unique strings of a binary string file (orc_load_strings_bin)."""
+    n = C.c_size_t(0)
+    if lib().orc_load_strings_bin(path.encode(), L, None, 0, C.byref(n)) != 0:
+        raise ValueError(f"orc_load_strings_bin({path}) failed")
+    out = np.zeros(max(n.value, 1), np.uint64)
+    lib().orc_load_strings_bin(path.encode(), L, out.ctypes.data, n.value, C.byref(n))
+    return out[: n.value]
 
 
 def excitations(bra: np.ndarray, ket: np.ndarray, L: int, ndiff: int, spin: int):

@@ -6,6 +6,9 @@
 //   ndet, helper_s (MakeHelpers + RemakeHelpers, tpb/helper.h:710-1226), hii_s
 //   (makeQChamDiagTerms), sigma_s (seconds of each of --reps mult calls), threads.
 // Usage: ref_bench --fcidump F --adetfile A [--bdetfile B] [--amax M] [--reps K]
+//        ref_bench --parse FILE --norb L [--reps K]
+//   times LoadAlphaDets (basic/makedeterminants.h:160-186: read, from_string or DecodeAlphaDets,
+//   sort_bitarray) on a string file alone and prints nstrings and parse_s (seconds per call).
 #include <chrono>
 #include <cmath>
 #include <deque>
@@ -23,8 +26,12 @@ int main(int argc, char **argv) {
   std::string fcidumpfile, adetfile, bdetfile;
   size_t amax = 0, bit_length = 20;
   int reps = 1;
+  std::string parsefile;
+  size_t parse_norb = 0;
   for (int i = 1; i < argc; ++i) {
     std::string a(argv[i]);
+    if (a == "--parse") parsefile = argv[++i];
+    else if (a == "--norb") parse_norb = std::strtoul(argv[++i], nullptr, 10);
     if (a == "--fcidump") fcidumpfile = argv[++i];
     else if (a == "--adetfile") adetfile = argv[++i];
     else if (a == "--bdetfile") bdetfile = argv[++i];
@@ -33,6 +40,20 @@ int main(int argc, char **argv) {
   }
   int provided;
   MPI_Init_thread(&argc, &argv, MPI_THREAD_FUNNELED, &provided);
+  if (!parsefile.empty()) {
+    std::vector<std::vector<size_t>> d;
+    std::string ts;
+    for (int r = 0; r < reps; ++r) {
+      d.clear();
+      auto p0 = std::chrono::steady_clock::now();
+      sbd::LoadAlphaDets(parsefile, d, bit_length, parse_norb);
+      auto p1 = std::chrono::steady_clock::now();
+      ts += (r ? "," : "") + std::to_string(std::chrono::duration<double>(p1 - p0).count());
+    }
+    std::printf("nstrings=%zu parse_s=%s\n", d.size(), ts.c_str());
+    MPI_Finalize();
+    return 0;
+  }
   sbd::FCIDump fcidump = sbd::LoadFCIDump(fcidumpfile);
   int L = 0, N = 0;
   double I0 = 0.0;

@@ -185,6 +185,43 @@ static int cmp_u64(const void *a, const void *b) {
 
 void orc_sort_strings(uint64_t *s, size_t n) { qsort(s, n, sizeof(uint64_t), cmp_u64); }
 
+int orc_load_strings_bin(const char *path, int L, uint64_t *out, size_t cap, size_t *n) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return -1;
+  const int rb = (L + 7) / 8;
+  unsigned char rec[8];
+  uint64_t *tmp = NULL;
+  size_t cnt = 0, tcap = 0;
+  int seq[64];
+  while (fread(rec, 1, (size_t)rb, f) == (size_t)rb) {
+    /* bits of the record from the high end of each byte; the first 8*rb - L are skipped */
+    int nb = 0, bit_index = 0;
+    for (int b = 0; b < rb; b++)
+      for (int i = 7; i >= 0; i--) {
+        if (8 * rb - L <= bit_index) seq[nb++] = (rec[b] >> i) & 1;
+        bit_index++;
+      }
+    /* reversed: orbital p is seq[L-1-p] */
+    uint64_t v = 0;
+    for (int p = 0; p < L; p++)
+      if (seq[L - 1 - p]) v |= (uint64_t)1 << p;
+    if (cnt == tcap) {
+      tcap = tcap ? 2 * tcap : 1024;
+      tmp = realloc(tmp, tcap * sizeof(uint64_t));
+    }
+    tmp[cnt++] = v;
+  }
+  fclose(f);
+  orc_sort_strings(tmp, cnt);
+  size_t u = 0;
+  for (size_t i = 0; i < cnt; i++)
+    if (u == 0 || tmp[i] != tmp[u - 1]) tmp[u++] = tmp[i];
+  *n = u;
+  if (out) memcpy(out, tmp, (u < cap ? u : cap) * sizeof(uint64_t));
+  free(tmp);
+  return 0;
+}
+
 int orc_load_strings(const char *path, int L, uint64_t *out, size_t cap, size_t *n) {
   FILE *f = fopen(path, "r");
   if (!f) return -1;

@@ -46,6 +46,12 @@ void orc_free_ham(orc_ham *h);
  * With out == NULL only the count is returned in *n.  Returns 0, or -1 on open failure,
  * -2 on a line longer than 64 orbitals or with characters other than 0/1. */
 int orc_load_strings(const char *path, int L, uint64_t *out, size_t cap, size_t *n);
+/* Binary string file (DecodeAlphaDets, basic/makedeterminants.h:63-108): records of
+ * ceil(L/8) bytes read while whole, bits taken from the most significant end of each byte, the
+ * first 8*ceil(L/8) - L skipped, the remaining L reversed so the last bit read is orbital 0; then
+ * sorted and made unique as the text reader does.  With out == NULL only the count is returned.
+ * Returns 0 or -1 on open failure. */
+int orc_load_strings_bin(const char *path, int L, uint64_t *out, size_t cap, size_t *n);
 /* Ascending sort as an unsigned integer (sort_bitarray / less_from_back). */
 void orc_sort_strings(uint64_t *s, size_t n);
 

@@ -5,6 +5,7 @@
 // ABI and nothing exits the process (the reference throws, exit()s or MPI_Abort()s instead:
 // tpb/helper.h:342-345, framework/fcidump.h:34-35, framework/cuda_utility.h:21-28).
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cstring>
 #include <new>
@@ -129,6 +130,7 @@ int sbd_tpb_destroy(sbd_tpb_handle *h) {
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->ev_co)
     if (e) cudaEventDestroy(e);
+  if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return SBD_TPB_OK;
@@ -367,6 +369,50 @@ int sbd_tpb_rdm(sbd_tpb_handle *h, const double *W, double *one, double *two, in
   TPB_CUDA(cudaStreamSynchronize(h->stream));
   return rdm_sep(h, h->d_tmp64, one, two, nullptr);
 }
+
+int sbd_tpb_parse_strings(sbd_tpb_handle *h, const void *bytes, size_t nbytes, int format, int norb, uint64_t *out,
+                          size_t cap, size_t *count) {
+  TPB_HANDLE(h);
+  if (!count) return fail(SBD_TPB_ERR_INVALID, "null count");
+  return parse_strings_device(h, bytes, nbytes, format, norb, out, cap, count, &h->last_parse_ms);
+}
+
+int sbd_tpb_read_strings(sbd_tpb_handle *h, const char *path, int norb, uint64_t *out, size_t cap, size_t *count) {
+  TPB_HANDLE(h);
+  if (!path || !count) return fail(SBD_TPB_ERR_INVALID, "null path/count");
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(SBD_TPB_ERR_IO, std::string("cannot open ") + path);
+  std::fseek(f, 0, SEEK_END);
+  const long sz = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  if (sz < 0) {
+    std::fclose(f);
+    return fail(SBD_TPB_ERR_IO, std::string("cannot size ") + path);
+  }
+  // pinned staging (kept on the handle) so the copy to HBM runs at link speed
+  if (h->stage_cap < (size_t)sz + 1) {
+    if (h->h_stage) cudaFreeHost(h->h_stage);
+    h->h_stage = nullptr;
+    h->stage_cap = 0;
+    if (cudaMallocHost(&h->h_stage, (size_t)sz + 1) != cudaSuccess) {
+      cudaGetLastError();
+      h->h_stage = nullptr;
+      std::fclose(f);
+      return fail(SBD_TPB_ERR_OOM, "pinned staging for the string file");
+    }
+    h->stage_cap = (size_t)sz + 1;
+  }
+  void *buf = h->h_stage;
+  const size_t got = sz ? std::fread(buf, 1, (size_t)sz, f) : 0;
+  std::fclose(f);
+  if (got != (size_t)sz) return fail(SBD_TPB_ERR_IO, std::string("short read of ") + path);
+  const std::string p(path);
+  const int format = (p.size() >= 4 && p.compare(p.size() - 4, 4, ".bin") == 0) ? SBD_TPB_STRINGS_BINARY
+                                                                                   : SBD_TPB_STRINGS_TEXT;
+  return parse_strings_device(h, buf, got, format, norb, out, cap, count, &h->last_parse_ms);
+}
+
+double sbd_tpb_last_parse_ms(sbd_tpb_handle *h) { return h ? (double)h->last_parse_ms : 0.0; }
 
 int sbd_tpb_carryover_strings(sbd_tpb_handle *h, const double *W, int mem, sbd_tpb_carryover *co) {
   TPB_HANDLE(h);

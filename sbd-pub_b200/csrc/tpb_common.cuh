@@ -126,6 +126,9 @@ struct sbd_tpb_handle {
   int sigma_kernels = 0;  // kernels timed in the last sigma (ev0, ev_k[0..], ev1)
   cudaEvent_t ev_co[2] = {nullptr, nullptr};  // around the weight pass of the last carry-over
   float last_carryover_ms[2] = {0.f, 0.f};    // weight pass, whole call
+  float last_parse_ms = 0.f;                   // last string-file parse (copy, parse, sort)
+  void *h_stage = nullptr;                     // pinned staging of string files (grow-only)
+  size_t stage_cap = 0;
   int num_sms = 148;
   size_t smem_optin = 0;
 
@@ -184,6 +187,10 @@ struct sbd_tpb_handle {
 };
 
 namespace sbdtpb {
+// strings.cu: parse/sort/unique a string file held in host memory; ms (may be null) receives the
+// device time from the copy to the last kernel
+int parse_strings_device(sbd_tpb_handle *h, const void *host_bytes, size_t nbytes, int format, int norb,
+                         uint64_t *out, size_t cap, size_t *count, float *ms);
 // carryover.cu: carry-over strings of a device vector (either sign convention)
 int carryover_device(sbd_tpb_handle *h, const double *dW, sbd_tpb_carryover *co);
 // tables.cu

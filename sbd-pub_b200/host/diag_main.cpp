@@ -115,9 +115,28 @@ int main(int argc, char **argv) {
   if (!tpbio::load_fcidump(fcidumpfile, fd, &err)) die(err);
   const int L = fd.norb;
   std::vector<uint64_t> adet, bdet;
-  if (!tpbio::load_strings(adetfile, L, adet, &err)) die(err);
-  if (bdetfile.empty()) bdet = adet;
-  else if (!tpbio::load_strings(bdetfile, L, bdet, &err)) die(err);
+  // string files (text or .bin, as LoadAlphaDets reads them) parsed, sorted and de-duplicated on
+  // the GPU
+  {
+    sbd_tpb_handle *sh = nullptr;
+    if (sbd_tpb_create(prm.device, &sh)) die(sbd_tpb_last_error());
+    auto read = [&](const std::string &path, std::vector<uint64_t> &out) {
+      std::ifstream f(path, std::ios::binary | std::ios::ate);
+      if (!f) die("Failed to open alpha det file: " + path);
+      const size_t bytes = (size_t)f.tellg();
+      const bool bin = path.size() >= 4 && path.compare(path.size() - 4, 4, ".bin") == 0;
+      const size_t cap = bin ? bytes / ((L + 7) / 8) : bytes / (L + 1) + 1;
+      out.resize(std::max<size_t>(cap, 1));
+      size_t n = 0;
+      if (sbd_tpb_read_strings(sh, path.c_str(), L, out.data(), out.size(), &n)) die(sbd_tpb_last_error());
+      out.resize(n);
+      if (out.empty()) die("no strings in " + path);
+    };
+    read(adetfile, adet);
+    if (bdetfile.empty()) bdet = adet;
+    else read(bdetfile, bdet);
+    sbd_tpb_destroy(sh);
+  }
   if (do_shuffle) {
     tpbio::shuffle_strings(adet, 1729);
     tpbio::shuffle_strings(bdet, 137);

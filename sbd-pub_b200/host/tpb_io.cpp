@@ -100,41 +100,6 @@ bool load_fcidump(const std::string &path, FciDump &out, std::string *err) {
   return true;
 }
 
-bool load_strings(const std::string &path, int norb, std::vector<uint64_t> &out, std::string *err) {
-  std::ifstream in(path);
-  if (!in.is_open()) {
-    if (err) *err = "Failed to open alpha det file: " + path;
-    return false;
-  }
-  if (path.size() >= 4 && path.substr(path.size() - 4) == ".bin") {
-    if (err) *err = "binary string files are not supported; use the .txt form";
-    return false;
-  }
-  out.clear();
-  std::string line;
-  while (std::getline(in, line)) {
-    while (!line.empty() && (line.back() == '\r' || line.back() == ' ')) line.pop_back();
-    if (line.empty()) continue;
-    if ((int)line.size() < norb) {
-      if (err) *err = "string shorter than NORB: '" + line + "'";
-      return false;
-    }
-    uint64_t v = 0;
-    for (int i = 0; i < norb; i++) {
-      const char c = line[norb - 1 - i];
-      if (c == '1') v |= 1ull << i;
-      else if (c != '0') {
-        if (err) *err = "string with characters other than 0/1: '" + line + "'";
-        return false;
-      }
-    }
-    out.push_back(v);
-  }
-  std::sort(out.begin(), out.end());
-  out.erase(std::unique(out.begin(), out.end()), out.end());
-  return true;
-}
-
 std::string make_string(uint64_t s, int norb) {
   std::string r(norb, '0');
   for (int i = 0; i < norb; i++)

@@ -20,10 +20,6 @@ struct FciDump {
 // it.  Returns false with *err set on failure.
 bool load_fcidump(const std::string &path, FciDump &out, std::string *err);
 
-// One string per line, orbital 0 is the last character (framework/bit_manipulation.h:215-230);
-// sorted ascending and duplicates removed (sort_bitarray, bit_manipulation.h:381-392).
-bool load_strings(const std::string &path, int norb, std::vector<uint64_t> &out, std::string *err);
-
 // Text form of a string as sbd::makestring prints it (orbital norb-1 first).
 std::string make_string(uint64_t s, int norb);
 

@@ -45,7 +45,9 @@ EXPORTED = [
     "sbd_tpb_precond_get_params", "sbd_tpb_precond_set_params", "sbd_tpb_precond_gradients",
     "sbd_tpb_precond_apply", "sbd_tpb_set_preconditioner", "sbd_tpb_carryover_strings",
     "sbd_tpb_carryover_capacity", "sbd_tpb_last_carryover_ms", "sbd_tpb_lanczos",
+    "sbd_tpb_parse_strings", "sbd_tpb_read_strings", "sbd_tpb_last_parse_ms",
 ]
+STRINGS_TEXT, STRINGS_BINARY = 0, 1
 CARRYOVER_NONE, CARRYOVER_DOMINANT, CARRYOVER_DOMINANT_SINGLES, CARRYOVER_CUTOFF_SINGLES = 0, 1, 2, 3
 ERR_CAPACITY = -8
 MLP_HIDDEN, MLP_FEATURES, MLP_PARAMS = 256, 64, 82689
@@ -127,6 +129,11 @@ def lib():
     L.sbd_tpb_davidson.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
     L.sbd_tpb_rdm.argtypes = [vp, vp, vp, vp, C.c_int]
     L.sbd_tpb_lanczos.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(Result)]
+    L.sbd_tpb_parse_strings.argtypes = [vp, vp, C.c_size_t, C.c_int, C.c_int, vp, C.c_size_t,
+                                        C.POINTER(C.c_size_t)]
+    L.sbd_tpb_read_strings.argtypes = [vp, C.c_char_p, C.c_int, vp, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.sbd_tpb_last_parse_ms.restype = C.c_double
+    L.sbd_tpb_last_parse_ms.argtypes = [vp]
     L.sbd_tpb_stream.restype = vp
     L.sbd_tpb_stream.argtypes = [vp]
     L.sbd_tpb_last_sigma_ms.restype = C.c_double
@@ -357,6 +364,29 @@ class Handle:
             ptr = W if isinstance(W, int) else W.data_ptr()
         _check(lib().sbd_tpb_carryover_strings(self.h, ptr, mem, C.byref(co)))
         return self._carryover_result(co, bufs)
+
+    def parse_strings(self, data, norb: int, fmt: int = STRINGS_TEXT) -> np.ndarray:
+        """Sorted unique strings of a string file's bytes, parsed on the GPU (sbd_tpb_parse_strings)."""
+        buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else data
+        buf = np.ascontiguousarray(buf, np.uint8)
+        cap = (len(buf) // ((norb + 7) // 8)) if fmt == STRINGS_BINARY else len(buf) // (norb + 1) + 1
+        out = np.zeros(max(cap, 1), np.uint64)
+        n = C.c_size_t(0)
+        _check(lib().sbd_tpb_parse_strings(self.h, buf.ctypes.data if len(buf) else None, len(buf), fmt, norb,
+                                           out.ctypes.data, len(out), C.byref(n)))
+        return out[: n.value].copy()
+
+    def read_strings(self, path: str, norb: int) -> np.ndarray:
+        """Sorted unique strings of a .txt or .bin string file, parsed on the GPU (sbd_tpb_read_strings)."""
+        size = os.path.getsize(path)
+        cap = size // ((norb + 7) // 8) if path.endswith(".bin") else size // (norb + 1) + 1
+        out = np.zeros(max(cap, 1), np.uint64)
+        n = C.c_size_t(0)
+        _check(lib().sbd_tpb_read_strings(self.h, path.encode(), norb, out.ctypes.data, len(out), C.byref(n)))
+        return out[: n.value].copy()
+
+    def last_parse_ms(self) -> float:
+        return float(lib().sbd_tpb_last_parse_ms(self.h))
 
     def last_carryover_ms(self):
         """(weight pass ms, whole call ms) of the last carry-over on this handle."""

@@ -161,10 +161,56 @@ def run_case(name: str, spec: dict, out_dir: str):
         return meta
 
 
+def write_bin_strings(path, strings, L, rng):
+    """Binary string file as DecodeAlphaDets reads it: ceil(L/8)-byte big-endian records, the
+    string in the low L bits, random bits in the unused high bits (which the reader skips)."""
+    rb = (L + 7) // 8
+    with open(path, "wb") as f:
+        for s in strings:
+            pad = int(rng.integers(0, 1 << (8 * rb - L))) << L if 8 * rb > L else 0
+            f.write((int(s) | pad).to_bytes(rb, "big"))
+
+
+def make_strings_fixture(out_dir):
+    """tests/golden/strings.npz: text and binary string files (unsorted, with duplicates, CRLF
+    line ends in one of them) and the strings the reference's LoadAlphaDets makes of them
+    (astr.u64 of ref_dump: from_string / DecodeAlphaDets, then sort_bitarray)."""
+    rng = np.random.default_rng(4242)
+    data, meta = {}, {}
+    for L, ne, cnt in ((12, 5, 300), (20, 7, 400), (36, 9, 500)):
+        pool = synth.sample_strings(L, ne, cnt, seed=L)
+        strs = [int(pool[i]) for i in rng.integers(0, len(pool), size=cnt + cnt // 3)]  # duplicates
+        with tempfile.TemporaryDirectory() as tmp:
+            h1, eri, core = synth.synthetic_hamiltonian(L, seed=L)
+            fd = os.path.join(tmp, "fcidump.txt")
+            synth.write_fcidump(fd, L, 2 * ne, h1, eri, core)
+            ftxt, fbin = os.path.join(tmp, "a.txt"), os.path.join(tmp, "a.bin")
+            eol = "\r\n" if L == 20 else "\n"
+            with open(ftxt, "w", newline="") as f:
+                for s_ in strs:
+                    f.write(format(s_, f"0{L}b") + eol)
+            write_bin_strings(fbin, strs, L, rng)
+            for kind, path in (("txt", ftxt), ("bin", fbin)):
+                d = os.path.join(tmp, kind)
+                os.makedirs(d)
+                subprocess.run([DUMP, "--fcidump", fd, "--adetfile", path, "--out", d], check=True,
+                               stdout=subprocess.DEVNULL)
+                data[f"L{L}_{kind}_bytes"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+                data[f"L{L}_{kind}_ref"] = np.fromfile(os.path.join(d, "astr.u64"), np.uint64)
+        meta[f"L{L}"] = dict(electrons=ne, lines=len(strs), unique=int(len(set(strs))))
+    np.savez_compressed(os.path.join(out_dir, "strings.npz"), **data)
+    return meta
+
+
 def main():
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + ["strings"]
     index_path = os.path.join(HERE, "cases.json")
     index = json.load(open(index_path)) if os.path.exists(index_path) else {}
+    if "strings" in names:
+        names = [n for n in names if n != "strings"]
+        print("case strings", flush=True)
+        index["strings"] = make_strings_fixture(HERE)
+        json.dump(index, open(index_path, "w"), indent=1, sort_keys=True)
     for name in names:
         print("case", name, flush=True)
         index[name] = run_case(name, CASES[name], HERE)
