@@ -194,8 +194,10 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       ra.m = ib + 1;
       ra.e_shifted = E[0];
       ra.e0 = E[0] + shift;
+      // FP32 vectors: the correction's denominator from H_ii - H_00 in FP32 (half the bytes of the
+      // FP64 diagonal; its 1e-7 relative rounding is far below what a preconditioner needs)
       ra.hii = h->d_hii;
-      ra.hii32 = nullptr;
+      ra.hii32 = std::is_same<T, float>::value ? h->d_hii32 : nullptr;
       // W is needed for the restart after the last step of a cycle; otherwise it is formed
       // only once, when the loop stops.  The last step of a cycle needs no correction.
       const bool last = ib == nb - 1;

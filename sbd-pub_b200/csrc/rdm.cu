@@ -42,40 +42,77 @@ __device__ __forceinline__ double block_sum(double x, double *red) {
   return s;  // valid in thread 0
 }
 
-// rho_a[Ia] and M[p][q]; one CTA per alpha row
+// rho_a[Ia] = sum_Ib W^2 and Y[Ia][q] = sum_{Ib : q in Ib} W^2; one CTA per alpha row.  Each warp
+// takes 32 beta columns at a time: the orbitals every lane's string holds get the warp's total
+// once, the others (held by some lanes only) one warp sum each; lane 0 adds them into its warp's
+// own row of shared memory, and the warps' rows are added in warp order, so the sums are the same
+// on every run (no floating-point atomics).
 __global__ void __launch_bounds__(kRdmThreads)
-    rdm_row_kernel(const double *__restrict__ W, const uint64_t *__restrict__ astr,
-                   const uint64_t *__restrict__ bstr, uint32_t nb, int L,
-                   double *__restrict__ rho_a, double *__restrict__ M) {
-  __shared__ double mq[64];
+    rdm_row_kernel(const double *__restrict__ W, const uint64_t *__restrict__ bstr, uint32_t nb, int L,
+                   double *__restrict__ rho_a, double *__restrict__ Y) {
+  __shared__ double mq[kRdmThreads / 32][64];
   __shared__ double red[32];
   const uint32_t ia = blockIdx.x;
-  if (threadIdx.x < 64) mq[threadIdx.x] = 0.0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < (kRdmThreads / 32) * 64; i += blockDim.x) (&mq[0][0])[i] = 0.0;
   __syncthreads();
   double s = 0.0;
-  for (uint32_t ib = threadIdx.x; ib < nb; ib += blockDim.x) {
-    const double w = W[(size_t)ia * nb + ib];
+  const uint32_t nbp = (nb + 31) & ~31u;  // every lane of a warp runs the same iterations
+  for (uint32_t ib = threadIdx.x; ib < nbp; ib += blockDim.x) {
+    const bool in = ib < nb;
+    const double w = in ? W[(size_t)ia * nb + ib] : 0.0;
     const double w2 = w * w;
+    const uint64_t occ = in ? bstr[ib] : 0ull;
     s += w2;
-    uint64_t occ = bstr[ib];
-    while (occ) {
-      atomicAdd(&mq[lowest_bit(occ)], w2);
-      occ &= occ - 1;
+    const unsigned lo = (unsigned)occ, hi = (unsigned)(occ >> 32);
+    const uint64_t all = ((uint64_t)__reduce_and_sync(0xffffffffu, hi) << 32) | __reduce_and_sync(0xffffffffu, lo);
+    const uint64_t any = ((uint64_t)__reduce_or_sync(0xffffffffu, hi) << 32) | __reduce_or_sync(0xffffffffu, lo);
+    double tot = w2;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    uint64_t some = any & ~all;
+    while (some) {
+      const int q = lowest_bit(some);
+      double v = ((occ >> q) & 1) ? w2 : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) mq[wid][q] += v;
+      some &= some - 1;
+    }
+    if (lane == 0) {
+      uint64_t a = all;
+      while (a) {
+        mq[wid][lowest_bit(a)] += tot;
+        a &= a - 1;
+      }
     }
   }
-  const double tot = block_sum(s, red);
-  if (threadIdx.x == 0) rho_a[ia] = tot;
+  const double t = block_sum(s, red);
+  if (threadIdx.x == 0) rho_a[ia] = t;
   __syncthreads();
-  uint64_t pa = astr[ia];
-  while (pa) {
-    const int p = lowest_bit(pa);
-    for (int q = threadIdx.x; q < L; q += blockDim.x) atomicAdd(&M[p * L + q], mq[q]);
-    pa &= pa - 1;
+  for (int q = threadIdx.x; q < L; q += blockDim.x) {
+    double v = 0.0;
+    for (int w = 0; w < kRdmThreads / 32; w++) v += mq[w][q];
+    Y[(size_t)ia * L + q] = v;
   }
 }
 
+// Mpart[c][p*L + q] = sum over alpha rows Ia of chunk c with p in Ia of Y[Ia][q]
+__global__ void rdm_pq_kernel(const double *__restrict__ Y, const uint64_t *__restrict__ astr, uint32_t na, int L,
+                              uint32_t rows_per_chunk, double *__restrict__ Mpart) {
+  const int pq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pq >= L * L) return;
+  const int p = pq / L, q = pq - p * L;
+  const uint32_t r0 = blockIdx.y * rows_per_chunk, r1 = min(na, r0 + rows_per_chunk);
+  double v = 0.0;
+  for (uint32_t r = r0; r < r1; r++)
+    if ((astr[r] >> p) & 1) v += Y[(size_t)r * L + q];
+  Mpart[(size_t)blockIdx.y * L * L + pq] = v;
+}
+
+// column sums of W^2 over a chunk of rows: part[chunk][col]
 __global__ void rdm_colsum_kernel(const double *__restrict__ W, uint32_t na, uint32_t nb,
-                                  uint32_t rows_per_chunk, double *__restrict__ rho_b) {
+                                  uint32_t rows_per_chunk, double *__restrict__ part) {
   const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= nb) return;
   const uint32_t r0 = blockIdx.y * rows_per_chunk;
@@ -85,7 +122,17 @@ __global__ void rdm_colsum_kernel(const double *__restrict__ W, uint32_t na, uin
     const double w = W[(size_t)r * nb + col];
     s += w * w;
   }
-  atomicAdd(&rho_b[col], s);
+  part[(size_t)blockIdx.y * nb + col] = s;
+}
+
+// rho_b[col] = sum of the chunk partials in chunk order
+__global__ void rdm_chunk_sum_kernel(const double *__restrict__ part, uint32_t nchunks, uint32_t n,
+                                     double *__restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (uint32_t c = 0; c < nchunks; c++) s += part[(size_t)c * n + i];
+  out[i] = s;
 }
 
 // T0[e] = sum_c X[bra,c] X[ket,c]; Tq[e][q] = same restricted to columns whose other-spin string
@@ -217,29 +264,39 @@ int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double
   const int L = h->L;
   const size_t n = h->ndet();
   Rdm R(L);
-  // ---- diagonal part
-  double *d_rho_a = nullptr, *d_rho_b = nullptr, *d_M = nullptr;
+  // ---- diagonal part (deterministic: fixed summation order throughout)
+  constexpr uint32_t kChunk = 1024;
+  const uint32_t nca = (na + kChunk - 1) / kChunk;
+  double *d_rho_a = nullptr, *d_rho_b = nullptr, *d_Y = nullptr, *d_Mp = nullptr, *d_cp = nullptr;
   TPB_CUDA(cudaMalloc(&d_rho_a, sizeof(double) * na));
   TPB_CUDA(cudaMalloc(&d_rho_b, sizeof(double) * nb));
-  TPB_CUDA(cudaMalloc(&d_M, sizeof(double) * L * L));
-  TPB_CUDA(cudaMemsetAsync(d_rho_b, 0, sizeof(double) * nb, h->stream));
-  TPB_CUDA(cudaMemsetAsync(d_M, 0, sizeof(double) * L * L, h->stream));
-  rdm_row_kernel<<<na, kRdmThreads, 0, h->stream>>>(W, h->d_astr, h->d_bstr, nb, L, d_rho_a, d_M);
+  TPB_CUDA(cudaMalloc(&d_Y, sizeof(double) * (size_t)na * L));
+  TPB_CUDA(cudaMalloc(&d_Mp, sizeof(double) * (size_t)nca * L * L));
+  TPB_CUDA(cudaMalloc(&d_cp, sizeof(double) * (size_t)nca * nb));
+  rdm_row_kernel<<<na, kRdmThreads, 0, h->stream>>>(W, h->d_bstr, nb, L, d_rho_a, d_Y);
   TPB_LAUNCHED(h);
   {
-    const uint32_t chunk = 256;
-    dim3 grid((nb + 255) / 256, (na + chunk - 1) / chunk);
-    rdm_colsum_kernel<<<grid, 256, 0, h->stream>>>(W, na, nb, chunk, d_rho_b);
+    dim3 grid((L * L + 127) / 128, nca);
+    rdm_pq_kernel<<<grid, 128, 0, h->stream>>>(d_Y, h->d_astr, na, L, kChunk, d_Mp);
+    TPB_LAUNCHED(h);
+    dim3 gridc((nb + 255) / 256, nca);
+    rdm_colsum_kernel<<<gridc, 256, 0, h->stream>>>(W, na, nb, kChunk, d_cp);
+    TPB_LAUNCHED(h);
+    rdm_chunk_sum_kernel<<<(nb + 255) / 256, 256, 0, h->stream>>>(d_cp, nca, nb, d_rho_b);
     TPB_LAUNCHED(h);
   }
-  std::vector<double> rho_a(na), rho_b(nb), M((size_t)L * L);
+  std::vector<double> rho_a(na), rho_b(nb), Mp((size_t)nca * L * L), M((size_t)L * L, 0.0);
   TPB_CUDA(cudaMemcpyAsync(rho_a.data(), d_rho_a, sizeof(double) * na, cudaMemcpyDeviceToHost, h->stream));
   TPB_CUDA(cudaMemcpyAsync(rho_b.data(), d_rho_b, sizeof(double) * nb, cudaMemcpyDeviceToHost, h->stream));
-  TPB_CUDA(cudaMemcpyAsync(M.data(), d_M, sizeof(double) * L * L, cudaMemcpyDeviceToHost, h->stream));
+  TPB_CUDA(cudaMemcpyAsync(Mp.data(), d_Mp, sizeof(double) * Mp.size(), cudaMemcpyDeviceToHost, h->stream));
   TPB_CUDA(cudaStreamSynchronize(h->stream));
+  for (uint32_t c = 0; c < nca; c++)
+    for (size_t k = 0; k < M.size(); k++) M[k] += Mp[(size_t)c * L * L + k];
   cudaFree(d_rho_a);
   cudaFree(d_rho_b);
-  cudaFree(d_M);
+  cudaFree(d_Y);
+  cudaFree(d_Mp);
+  cudaFree(d_cp);
   auto diag_same = [&](int s, const std::vector<uint64_t> &str, const std::vector<double> &rho) {
     for (size_t i = 0; i < str.size(); i++) {
       const double w2 = rho[i];

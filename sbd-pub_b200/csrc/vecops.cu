@@ -150,8 +150,8 @@ struct ResidualBody {
       acc[0] += w[l] * w[l];
       acc[1] += r * r;
       if (a.t) {
-        const double hd = a.hii32 ? (double)__ldg(&a.hii32[i + l]) : __ldg(&a.hii[i + l]);
-        const double d = a.e0 - hd;
+        // E0 - H_ii, or with the FP32 diagonal (E0 - H_00) - (H_ii - H_00)
+        const double d = a.hii32 ? a.e_shifted - (double)__ldg(&a.hii32[i + l]) : a.e0 - __ldg(&a.hii[i + l]);
         tt[l] = (T)((fabs(d) > 1.0e-12) ? r / d : r / (d - 1.0e-12));
       }
     }

@@ -26,7 +26,7 @@ struct ResidualArgs {
   double e_shifted;   // Ritz value of (H - shift)
   double e0;          // Ritz value of H
   const double *hii;  // FP64 diagonal (FP64 vectors)
-  const float *hii32; // H_ii - H_00 in FP32 (FP32 vectors); e0 is then E - H_00
+  const float *hii32; // H_ii - H_00 in FP32 (FP32 vectors; used with e_shifted = E - H_00)
   T *W;               // Ritz vector out (may be null)
   T *t;               // preconditioned correction out (may be null: W only)
 };
