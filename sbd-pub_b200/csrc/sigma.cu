@@ -25,7 +25,17 @@ namespace {
 
 constexpr int kBlkRows = 8;  // bra rows per CTA
 constexpr int kBlkThreads = 128;
-
+// Thread mapping of a CTA per element type and pass: the 128 threads form G row groups, each
+// thread holding kBlkRows / G rows of VW columns (fewer accumulators per thread for larger G, so
+// more CTAs fit an SM), with the register budget of M CTAs per SM.  Measured at 4e8 determinants
+// (norb=32), ms per pass: FP32 alpha 1 group / 5 CTAs 6.38 (2/7: 6.47, 2/8 and 2/9 spill: 6.40;
+// 1/6: 6.42), FP32 beta 2/9 4.74 (1/5: 5.64, 2/7: 5.44, 2/8: 4.91, 2/10: 5.20), FP64 alpha 2/7
+// 8.36 (1/5: 10.23), FP64 beta 2/9 7.14 (1/5: 8.80, 2/8: 7.56).  Four groups lose the 16-byte runs
+// of the FP32 transposed write-out and run slower.  The FP32 alpha pass takes 1/5 only on large
+// problems: its 512-column slabs leave small ones with too few CTAs (norb=12 FCI, 924 x 924:
+// 0.84 ms against 0.48 with 2/7; 4,000 x 4,000: 1.31 against 1.16; 10,000 x 10,000: 3.10 against
+// 3.21), so it switches at 10,000 CTAs.
+// The mapping of a pass as template arguments: G row groups, register budget of M CTAs per SM.
 template <typename T>
 __device__ __forceinline__ T val_of(const double *v, const float *vf, uint32_t e);
 template <>
@@ -110,20 +120,23 @@ struct BlockArgs {
 };
 
 // One kernel, two passes.  A CTA owns kBlkRows consecutive bra strings (rows of X) and a slab of
-// kBlkThreads*VW columns, each thread VW consecutive columns (one 16-byte access when the row
-// length allows it).  Blocks run slab-major so the CTAs in flight gather from one slab of X that
-// stays in L2.  The block's table entries (one contiguous CSR range) are staged in shared memory
-// first, so the gathers X[ket, cols] issue back to back.
+// (kBlkThreads / G) * VW columns; its threads form G row groups, each thread VW consecutive
+// columns (one 16-byte access when the row length allows it) of kBlkRows / G rows.  Blocks run
+// slab-major so the CTAs in flight gather from one slab of X that stays in L2.  The block's table
+// entries (one contiguous CSR range) are staged in shared memory first, so the gathers
+// X[ket, cols] issue back to back.
 //   alpha pass (kAlpha): X = C.  Adds the diagonal and the alpha-single x beta-single terms and
 //     writes sigma[Ia, Ib] once; the thread's own C[Ia-block, cols] values go out transposed to
-//     C^T as kBlkRows-element contiguous runs.
-//   beta pass: X = C^T.  Each thread adds its kBlkRows x VW results into
-//     sigma[Ia, Ib0 .. Ib0+kBlkRows) (contiguous along Ib) for its columns Ia.
-template <typename T, bool kAlpha, bool kVec>
-__global__ void __launch_bounds__(kBlkThreads, 5)
+//     C^T as contiguous runs of its rows.
+//   beta pass: X = C^T.  Each thread adds its rows x VW results into sigma[Ia, Ib0 ...)
+//     (contiguous along Ib) for its columns Ia.
+template <typename T, bool kAlpha, bool kVec, int G, int M>
+__global__ void __launch_bounds__(kBlkThreads, M)
     sigma_block_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
   constexpr int VW = 16 / sizeof(T);
-  constexpr int W = kBlkThreads * VW;
+  constexpr int TC = kBlkThreads / G;  // threads across the columns of the slab
+  constexpr int RPT = kBlkRows / G;    // rows per thread
+  constexpr int W = TC * VW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *sd_ket = reinterpret_cast<uint32_t *>(smem_raw);
   T *sd_val = reinterpret_cast<T *>(smem_raw + ((a.max_d * 4 + 15) & ~15u));
@@ -139,7 +152,8 @@ __global__ void __launch_bounds__(kBlkThreads, 5)
   const uint32_t ncols = a.ncols;
   const int L = a.L, L2 = L * L;
   const int nr = (int)min((uint32_t)kBlkRows, a.nrows - r0);
-  const uint32_t cbase = slab * W + threadIdx.x * VW;  // first of this thread's VW columns
+  const int grp = threadIdx.x / TC;                                  // row group of this thread
+  const uint32_t cbase = slab * W + (threadIdx.x % TC) * VW;         // first of its VW columns
 
   // stage the block's table entries
   const uint32_t dlo = __ldg(&a.d_off[r0]), dhi = __ldg(&a.d_off[r0 + nr]);
@@ -165,20 +179,21 @@ __global__ void __launch_bounds__(kBlkThreads, 5)
   const bool any = ok[0];
   const bool full = ok[VW - 1];
 
-  T acc[kBlkRows][VW];
-  T own[kAlpha ? kBlkRows : 1][VW];
+  T acc[RPT][VW];
+  T own[kAlpha ? RPT : 1][VW];
 #pragma unroll
-  for (int r = 0; r < kBlkRows; r++) {
+  for (int r = 0; r < RPT; r++) {
 #pragma unroll
     for (int i = 0; i < VW; i++) {
       acc[r][i] = T(0);
       if (kAlpha) own[r][i] = T(0);
     }
   }
+  const int rlo = grp * RPT;  // this thread's rows: r0 + rlo .. r0 + rlo + RPT
 #pragma unroll
-  for (int r = 0; r < kBlkRows; r++) {
-    if (r >= nr || !any) continue;
-    const uint32_t row = r0 + r;
+  for (int r = 0; r < RPT; r++) {
+    if (rlo + r >= nr || !any) continue;
+    const uint32_t row = r0 + rlo + r;
     const uint32_t d0 = __ldg(&a.d_off[row]) - dlo, d1 = __ldg(&a.d_off[row + 1]) - dlo;
 #pragma unroll 4
     for (uint32_t e = d0; e < d1; e++) {
@@ -263,32 +278,37 @@ __global__ void __launch_bounds__(kBlkThreads, 5)
       }
     }
   }
-  // transposed write-out: column c gets rows r0 .. r0+nr contiguous (index c * nrows + r), as
+  // transposed write-out: column c gets this thread's rows contiguous (index c * nrows + r), as
   // 16-byte accesses when the block is full and every column starts 16-byte aligned
   constexpr int RW = 16 / sizeof(T);
-  const bool vec_out = kVec && nr == kBlkRows && (a.nrows % RW) == 0;
+  constexpr bool kRuns = RPT % RW == 0;  // the thread's rows form whole 16-byte runs
+  const bool vec_out = kRuns && kVec && nr == kBlkRows && (a.nrows % RW) == 0;
 #pragma unroll
   for (int i = 0; i < VW; i++) {
     if (!ok[i]) continue;
-    const size_t o = (size_t)(cbase + i) * a.nrows + r0;
-    if (vec_out) {
+    const size_t o = (size_t)(cbase + i) * a.nrows + r0 + rlo;
+    if constexpr (kRuns) {
+      if (vec_out) {
 #pragma unroll
-      for (int r = 0; r < kBlkRows; r += RW) {
-        Vec<T, RW, true> v;
-        if (kAlpha) {
+        for (int r = 0; r < RPT; r += RW) {
+          Vec<T, RW, true> v;
+          if (kAlpha) {
 #pragma unroll
-          for (int q = 0; q < RW; q++) v.v[q] = own[r + q][i];
-        } else {
-          v.load_rw(out + o + r);
+            for (int q = 0; q < RW; q++) v.v[q] = own[r + q][i];
+          } else {
+            v.load_rw(out + o + r);
 #pragma unroll
-          for (int q = 0; q < RW; q++) v.v[q] += acc[r + q][i];
+            for (int q = 0; q < RW; q++) v.v[q] += acc[r + q][i];
+          }
+          v.store(kAlpha ? XT + o + r : out + o + r);
         }
-        v.store(kAlpha ? XT + o + r : out + o + r);
+        continue;
       }
-    } else {
+    }
+    {
 #pragma unroll
-      for (int r = 0; r < kBlkRows; r++) {
-        if (r < nr) {
+      for (int r = 0; r < RPT; r++) {
+        if (rlo + r < nr) {
           if (kAlpha) XT[o + r] = own[r][i];
           else out[o + r] += acc[r][i];
         }
@@ -424,10 +444,10 @@ int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y) {
   return SBD_TPB_OK;
 }
 
-template <typename T, bool kAlpha>
-int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
+template <typename T, bool kAlpha, int G, int M>
+int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
   constexpr int VW = 16 / sizeof(T);
-  constexpr int W = kBlkThreads * VW;
+  constexpr int W = (kBlkThreads / G) * VW;
   const size_t nrb = (ba.nrows + kBlkRows - 1) / kBlkRows, nslab = (ba.ncols + W - 1) / W;
   const size_t blocks = nrb * nslab;
   if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
@@ -438,11 +458,25 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
                    (reinterpret_cast<uintptr_t>(out) % 16) == 0 &&
                    (!XT || (reinterpret_cast<uintptr_t>(XT) % 16) == 0);
-  auto kern = vec ? sigma_block_kernel<T, kAlpha, true> : sigma_block_kernel<T, kAlpha, false>;
+  auto kern = vec ? sigma_block_kernel<T, kAlpha, true, G, M> : sigma_block_kernel<T, kAlpha, false, G, M>;
   TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
   TPB_LAUNCHED(h);
   return SBD_TPB_OK;
+}
+
+template <typename T, bool kAlpha>
+int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
+  if constexpr (sizeof(T) == 4 && kAlpha) {
+    const size_t blocks_g1 =
+        ((ba.nrows + kBlkRows - 1) / kBlkRows) * ((ba.ncols + kBlkThreads * 4 - 1) / (kBlkThreads * 4));
+    if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 1, 5>(h, ba, X, out, XT);
+    return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
+  } else if constexpr (kAlpha) {
+    return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
+  } else {
+    return launch_block_cfg<T, kAlpha, 2, 9>(h, ba, X, out, XT);
+  }
 }
 
 // Most entries of any kBlkRows-row block of a CSR table (shared-memory staging size).
