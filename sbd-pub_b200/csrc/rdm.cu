@@ -136,38 +136,97 @@ __global__ void rdm_chunk_sum_kernel(const double *__restrict__ part, uint32_t n
 }
 
 // T0[e] = sum_c X[bra,c] X[ket,c]; Tq[e][q] = same restricted to columns whose other-spin string
-// holds q (only when Tq != null).  One CTA per bra row of the CSR table.
+// holds q (only when Tq != null).  One CTA per bra row of the CSR table; its entries go kPairE at a
+// time, so each pass over the columns reads the bra row once for kPairE ket rows.  The per-orbital
+// sums take the warp trick of rdm_row_kernel (orbitals held by all 32 columns of a warp get the
+// warp total, the others one warp sum each, lane 0 adds into its warp's row of shared memory), and
+// every sum has a fixed order, so the results repeat bit for bit.
+constexpr int kPairE = 4;
+
 __global__ void __launch_bounds__(kRdmThreads)
     rdm_pair_kernel(const double *__restrict__ X, uint32_t ncol, const uint32_t *__restrict__ off,
                     const uint32_t *__restrict__ ket, const uint64_t *__restrict__ other, int L,
                     double *__restrict__ T0, double *__restrict__ Tq) {
-  __shared__ double red[32];
-  __shared__ double acc[64];
+  constexpr int NW = kRdmThreads / 32;
+  __shared__ double red[NW][kPairE];
+  __shared__ double acc[kPairE][NW][64];
   const uint32_t row = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double *xr = X + (size_t)row * ncol;
-  for (uint32_t e = off[row]; e < off[row + 1]; e++) {
-    const double *xk = X + (size_t)ket[e] * ncol;
+  const uint32_t ncp = (ncol + 31) & ~31u;  // every lane of a warp runs the same iterations
+  for (uint32_t e0 = off[row]; e0 < off[row + 1]; e0 += kPairE) {
+    const int ne = (int)min((uint32_t)kPairE, off[row + 1] - e0);
+    const double *xk[kPairE];
+#pragma unroll
+    for (int k = 0; k < kPairE; k++) xk[k] = X + (size_t)ket[e0 + (k < ne ? k : 0)] * ncol;
     if (Tq) {
-      if (threadIdx.x < 64) acc[threadIdx.x] = 0.0;
+      for (int i = threadIdx.x; i < kPairE * NW * 64; i += blockDim.x) (&acc[0][0][0])[i] = 0.0;
       __syncthreads();
     }
-    double s = 0.0;
-    for (uint32_t c = threadIdx.x; c < ncol; c += blockDim.x) {
-      const double x = xr[c] * xk[c];
-      s += x;
+    double sum[kPairE];
+#pragma unroll
+    for (int k = 0; k < kPairE; k++) sum[k] = 0.0;
+    for (uint32_t c = threadIdx.x; c < ncp; c += blockDim.x) {
+      const bool in = c < ncol;
+      const double b = in ? xr[c] : 0.0;
+      double x[kPairE];
+#pragma unroll
+      for (int k = 0; k < kPairE; k++) {
+        x[k] = (in && k < ne) ? b * xk[k][c] : 0.0;
+        sum[k] += x[k];
+      }
       if (Tq) {
-        uint64_t occ = other[c];
-        while (occ) {
-          atomicAdd(&acc[lowest_bit(occ)], x);
-          occ &= occ - 1;
+        const uint64_t occ = in ? other[c] : 0ull;
+        const unsigned lo = (unsigned)occ, hi = (unsigned)(occ >> 32);
+        const uint64_t all =
+            ((uint64_t)__reduce_and_sync(0xffffffffu, hi) << 32) | __reduce_and_sync(0xffffffffu, lo);
+        const uint64_t any =
+            ((uint64_t)__reduce_or_sync(0xffffffffu, hi) << 32) | __reduce_or_sync(0xffffffffu, lo);
+#pragma unroll
+        for (int k = 0; k < kPairE; k++) {
+          if (k >= ne) break;
+          double tot = x[k];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+          uint64_t some = any & ~all;
+          while (some) {
+            const int q = lowest_bit(some);
+            double v = ((occ >> q) & 1) ? x[k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) acc[k][wid][q] += v;
+            some &= some - 1;
+          }
+          if (lane == 0) {
+            uint64_t a = all;
+            while (a) {
+              acc[k][wid][lowest_bit(a)] += tot;
+              a &= a - 1;
+            }
+          }
         }
       }
     }
-    const double tot = block_sum(s, red);
-    if (threadIdx.x == 0) T0[e] = tot;
+#pragma unroll
+    for (int k = 0; k < kPairE; k++) {
+      double v = sum[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[wid][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < ne) {
+      double t = 0.0;
+      for (int w = 0; w < NW; w++) t += red[w][threadIdx.x];
+      T0[e0 + threadIdx.x] = t;
+    }
     if (Tq) {
-      __syncthreads();
-      for (int q = threadIdx.x; q < L; q += blockDim.x) Tq[(size_t)e * L + q] = acc[q];
+      for (int i = threadIdx.x; i < ne * L; i += blockDim.x) {
+        const int k = i / L, q = i - k * L;
+        double t = 0.0;
+        for (int w = 0; w < NW; w++) t += acc[k][w][q];
+        Tq[(size_t)(e0 + k) * L + q] = t;
+      }
     }
     __syncthreads();
   }
