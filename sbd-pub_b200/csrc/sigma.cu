@@ -31,10 +31,13 @@ constexpr int kBlkThreads = 128;
 // (norb=32), ms per pass: FP32 alpha 1 group / 5 CTAs 6.38 (2/7: 6.47, 2/8 and 2/9 spill: 6.40;
 // 1/6: 6.42), FP32 beta 2/9 4.74 (1/5: 5.64, 2/7: 5.44, 2/8: 4.91, 2/10: 5.20), FP64 alpha 2/7
 // 8.36 (1/5: 10.23), FP64 beta 2/9 7.14 (1/5: 8.80, 2/8: 7.56).  Four groups lose the 16-byte runs
-// of the FP32 transposed write-out and run slower.  The FP32 alpha pass takes 1/5 only on large
-// problems: its 512-column slabs leave small ones with too few CTAs (norb=12 FCI, 924 x 924:
-// 0.84 ms against 0.48 with 2/7; 4,000 x 4,000: 1.31 against 1.16; 10,000 x 10,000: 3.10 against
-// 3.21), so it switches at 10,000 CTAs.
+// of the FP32 transposed write-out and run slower.  On large problems the FP32 alpha pass keeps one
+// group and parks the C values it writes out transposed in shared memory instead of 32 registers
+// (OS), which fits 7 CTAs per SM: 5.83 ms (registers, 5 CTAs: 6.36; parked, 5 or 6 CTAs: 6.49 /
+// 6.03; 8 CTAs spills: 6.56); parking gains nothing in FP64 (2/8: 8.17 at norb=32 but 4.20
+// against 3.83 at norb=28).  Its 512-column slabs leave small problems with too few CTAs (norb=12
+// FCI, 924 x 924: 0.84 ms against 0.48 with 2/7; 4,000 x 4,000: 1.31 against 1.16), so below
+// 10,000 CTAs it takes 2/7.
 // The mapping of a pass as template arguments: G row groups, register budget of M CTAs per SM.
 template <typename T>
 __device__ __forceinline__ T val_of(const double *v, const float *vf, uint32_t e);
@@ -130,7 +133,7 @@ struct BlockArgs {
 //     C^T as contiguous runs of its rows.
 //   beta pass: X = C^T.  Each thread adds its rows x VW results into sigma[Ia, Ib0 ...)
 //     (contiguous along Ib) for its columns Ia.
-template <typename T, bool kAlpha, bool kVec, int G, int M>
+template <typename T, bool kAlpha, bool kVec, int G, int M, bool OS>
 __global__ void __launch_bounds__(kBlkThreads, M)
     sigma_block_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
   constexpr int VW = 16 / sizeof(T);
@@ -145,6 +148,10 @@ __global__ void __launch_bounds__(kBlkThreads, M)
   uint32_t *ss_ket = reinterpret_cast<uint32_t *>(sp);
   int32_t *ss_pair = reinterpret_cast<int32_t *>(sp + a.max_s * 4);
   double *ss_val = reinterpret_cast<double *>(sp + ((a.max_s * 8 + 15) & ~15u));
+  // OS: the alpha pass parks its own C values for the transposed write-out in shared memory
+  // ([row][column of the thread][thread], conflict-free) instead of registers
+  T *own_s = reinterpret_cast<T *>(
+      (reinterpret_cast<uintptr_t>(ss_val + a.max_s) + 15) & ~(uintptr_t)15);
 
   const uint32_t nrb = (a.nrows + kBlkRows - 1) / kBlkRows;
   const uint32_t rb = blockIdx.x % nrb, slab = blockIdx.x / nrb;
@@ -180,13 +187,13 @@ __global__ void __launch_bounds__(kBlkThreads, M)
   const bool full = ok[VW - 1];
 
   T acc[RPT][VW];
-  T own[kAlpha ? RPT : 1][VW];
+  T own[(kAlpha && !OS) ? RPT : 1][VW];
 #pragma unroll
   for (int r = 0; r < RPT; r++) {
 #pragma unroll
     for (int i = 0; i < VW; i++) {
       acc[r][i] = T(0);
-      if (kAlpha) own[r][i] = T(0);
+      if (kAlpha && !OS) own[r][i] = T(0);
     }
   }
   const int rlo = grp * RPT;  // this thread's rows: r0 + rlo .. r0 + rlo + RPT
@@ -264,7 +271,8 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       }
 #pragma unroll
       for (int i = 0; i < VW; i++) {
-        own[r][i] = xo.v[i];
+        if (OS) own_s[(r * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
+        else own[r][i] = xo.v[i];
         double res = (double)acc[r][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
         if (a.accumulate) res += (double)ov.v[i];
         ov.v[i] = (T)res;
@@ -294,7 +302,8 @@ __global__ void __launch_bounds__(kBlkThreads, M)
           Vec<T, RW, true> v;
           if (kAlpha) {
 #pragma unroll
-            for (int q = 0; q < RW; q++) v.v[q] = own[r + q][i];
+            for (int q = 0; q < RW; q++)
+              v.v[q] = OS ? own_s[((r + q) * VW + i) * kBlkThreads + threadIdx.x] : own[OS ? 0 : r + q][i];
           } else {
             v.load_rw(out + o + r);
 #pragma unroll
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
 #pragma unroll
       for (int r = 0; r < RPT; r++) {
         if (rlo + r < nr) {
-          if (kAlpha) XT[o + r] = own[r][i];
+          if (kAlpha) XT[o + r] = OS ? own_s[(r * VW + i) * kBlkThreads + threadIdx.x] : own[OS ? 0 : r][i];
           else out[o + r] += acc[r][i];
         }
       }
@@ -444,7 +453,7 @@ int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y) {
   return SBD_TPB_OK;
 }
 
-template <typename T, bool kAlpha, int G, int M>
+template <typename T, bool kAlpha, int G, int M, bool OS = false>
 int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
   constexpr int VW = 16 / sizeof(T);
   constexpr int W = (kBlkThreads / G) * VW;
@@ -452,13 +461,14 @@ int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out,
   const size_t blocks = nrb * nslab;
   if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
   const size_t smem = ((ba.max_d * 4 + 15) & ~(size_t)15) + (size_t)ba.max_d * sizeof(T) + 16 +
-                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16;
+                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16 +
+                      (OS ? (size_t)(kBlkRows / G) * VW * kBlkThreads * sizeof(T) + 16 : 0);
   if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
   // 16-byte column accesses need every row of X to start 16-byte aligned
   const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
                    (reinterpret_cast<uintptr_t>(out) % 16) == 0 &&
                    (!XT || (reinterpret_cast<uintptr_t>(XT) % 16) == 0);
-  auto kern = vec ? sigma_block_kernel<T, kAlpha, true, G, M> : sigma_block_kernel<T, kAlpha, false, G, M>;
+  auto kern = vec ? sigma_block_kernel<T, kAlpha, true, G, M, OS> : sigma_block_kernel<T, kAlpha, false, G, M, OS>;
   TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
   TPB_LAUNCHED(h);
@@ -470,7 +480,7 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   if constexpr (sizeof(T) == 4 && kAlpha) {
     const size_t blocks_g1 =
         ((ba.nrows + kBlkRows - 1) / kBlkRows) * ((ba.ncols + kBlkThreads * 4 - 1) / (kBlkThreads * 4));
-    if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 1, 5>(h, ba, X, out, XT);
+    if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 1, 7, true>(h, ba, X, out, XT);
     return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
   } else if constexpr (kAlpha) {
     return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
