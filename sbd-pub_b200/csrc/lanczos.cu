@@ -1,16 +1,17 @@
 // Lanczos for the lowest root (--method 2): the reference's matrix-free Lanczos
 // (tpb/lanczos.h:167-320; dispatched from tpb/sbdiag.h:404-411), on the same sigma as Davidson.
 //
-// Per outer iteration, from the current W (not renormalised, as in the reference):
+// Per outer iteration, from the current W:
 //   C_0 = W, HC = 0
 //   step k: HC += H C_k; alpha_k = <C_k, HC>; lowest eigenvalues of the (k+1)x(k+1) tridiagonal
 //   T; stop when the lowest moved by less than eps; otherwise r = HC - alpha_k C_k,
 //   beta_k = |r|, C_{k+1} = r / beta_k, HC = -beta_k C_k (so the next sigma completes the
 //   three-term recurrence); end the iteration early when beta_k < eps.
 //   W = sum_k u_k C_k with u the lowest eigenvector of T.
-// There is no reorthogonalisation, as in the reference.  The vectors stay in HBM (FP64, separated
-// convention); each step is one accumulating sigma plus two fused vector passes and a dot, with
-// two host reads (alpha, beta^2).  T is tridiagonal, so its eigenvalues come from Sturm-sequence
+// There is no reorthogonalisation, as in the reference.  Unlike the reference, W is renormalised
+// after each outer iteration (see below); with orthonormal Krylov vectors its norm is 1 anyway.
+// The vectors stay in HBM (FP64, separated convention); each step is one accumulating sigma plus
+// two fused vector passes and a dot, with two host reads (alpha, beta^2).  T is tridiagonal, so its eigenvalues come from Sturm-sequence
 // bisection and the lowest eigenvector from inverse iteration with a pivoted tridiagonal
 // factorisation, instead of the reference's dense LAPACK dsyev on the same matrix (same
 // eigenvalues; the eigenvector's sign is fixed here by u_0 >= 0, where dsyev leaves it to the
@@ -252,6 +253,14 @@ int lanczos_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0, sb
     lz_scale_set_kernel<<<blocks, kLzThreads, 0, h->stream>>>(C[0].p, W.p, u[0], n);
     TPB_LAUNCHED(h);
     for (int k = 1; k < m; k++) TPB_CHECK(axpby<double>(h, C[k].p, W.p, u[k], 1.0, n));
+    // renormalised restart: without reorthogonalisation the Krylov vectors lose orthogonality once
+    // the lowest Ritz value converges, and the norm of sum_k u_k C_k drifts from 1; restarting from
+    // such a W biases the next alpha_0 = <W|H|W> and the drift grows at every restart
+    double ww = 0.0;
+    const double *wp[1] = {W.p};
+    TPB_CHECK(multi_dot<double>(h, wp, 1, W.p, n, &ww));
+    if (!(ww > 0.0)) return fail(SBD_TPB_ERR_NOT_CONVERGED, "lanczos: the Ritz vector vanished");
+    TPB_CHECK(scale_vec<double>(h, W.p, 1.0 / std::sqrt(ww), n));
     if (stop) {
       conv = 1;
       break;
