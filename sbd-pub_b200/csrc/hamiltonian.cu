@@ -203,6 +203,8 @@ void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->d_ab_rows);
   free_dev(h->d_ab_colp);
   free_dev(h->d_ab_bsp);
+  free_dev(h->d_ab_kets);
+  h->ab_nkets = 0;
   h->ab_nrows = h->ab_ncols = h->ab_max_k = 0;
   h->blk_for = nullptr;
   h->have_tables = false;

@@ -329,15 +329,19 @@ __global__ void __launch_bounds__(kBlkThreads, M)
 // Alpha-single x beta-single terms when both singles tables are sparse:
 //   sigma[Ia, Ib] += sum_{(Ja, pq, sa) in S_a(Ia)} sum_{(Jb, rs, sb) in S_b(Ib)} sa sb (pq|rs) C[Ja, Jb]
 // One CTA per alpha row Ia that has singles.  For a group of its singles the CTA stages in shared
-// memory the whole ket rows C[Ja] and the integral rows sa (pq|.) (sign folded in), so the
-// scattered reads C[Ja, Jb] and (pq|rs) at the beta singles are shared-memory reads; each thread
+// memory the ket rows C[Ja] -- only the columns Jb that are kets of some beta single, compacted
+// (kets[] lists them ascending; the beta program addresses them by position) -- and the integral
+// rows sa (pq|.) (sign folded in), so the scattered reads C[Ja, Jb] and (pq|rs) at the beta singles
+// are shared-memory reads; each thread
 // owns a set of beta columns Ib that have singles and adds its sum into sigma[Ia, Ib] once per
 // group.  Groups are sized so several CTAs fit on an SM.  Without room for one row (kStage
 // false) the same loop reads C and the integrals through L1/L2.
 struct AbSparseArgs {
   const uint32_t *rows;  // alpha rows with at least one single
   const uint2 *colp;     // beta columns with singles: (column, first entry), then (0, nnz)
-  const uint2 *bsp;      // beta singles entries: (ket, +-(rs + 1) with the beta sign)
+  const uint2 *bsp;      // beta singles entries: (position of the ket in kets, +-(rs + 1) with the beta sign)
+  const uint32_t *kets;  // [nk] the distinct kets of the beta singles, ascending
+  uint32_t nk;
   uint32_t ncols_s;
   const uint32_t *as_off, *as_ket;
   const int32_t *as_pair;  // +-(pq + 1), sign = alpha sign
@@ -351,8 +355,8 @@ template <typename T, bool kStage>
 __global__ void __launch_bounds__(256)
     ab_sparse_kernel(AbSparseArgs a, const T *__restrict__ C, T *__restrict__ sigma) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *rows = reinterpret_cast<T *>(smem_raw);                // [group][nb]
-  T *gint = rows + (size_t)a.group * a.nb;                  // [group][L2], sign folded in
+  T *rows = reinterpret_cast<T *>(smem_raw);                // [group][nk]
+  T *gint = rows + (size_t)a.group * a.nk;                  // [group][L2], sign folded in
   const uint32_t ia = __ldg(&a.rows[blockIdx.x]);
   const uint32_t e0 = __ldg(&a.as_off[ia]), e1 = __ldg(&a.as_off[ia + 1]);
   T *srow = sigma + (size_t)ia * a.nb;
@@ -362,8 +366,8 @@ __global__ void __launch_bounds__(256)
       __syncthreads();
       for (uint32_t j = 0; j < ng; j++) {
         const T *src = C + (size_t)__ldg(&a.as_ket[g0 + j]) * a.nb;
-        T *dst = rows + (size_t)j * a.nb;
-        for (uint32_t c = threadIdx.x; c < a.nb; c += blockDim.x) dst[c] = __ldg(&src[c]);
+        T *dst = rows + (size_t)j * a.nk;
+        for (uint32_t c = threadIdx.x; c < a.nk; c += blockDim.x) dst[c] = __ldg(&src[__ldg(&a.kets[c])]);
         const int32_t pa = __ldg(&a.as_pair[g0 + j]);
         const double *erow = a.eri + (size_t)((pa > 0 ? pa : -pa) - 1) * a.L2;
         T *gdst = gint + (size_t)j * a.L2;
@@ -387,11 +391,12 @@ __global__ void __launch_bounds__(256)
         double sum = 0.0;
         for (uint32_t j = 0; j < ng; j++) {
           if (kStage) {
-            sum += (double)gint[(size_t)j * a.L2 + rs] * (double)rows[(size_t)j * a.nb + jb];
+            sum += (double)gint[(size_t)j * a.L2 + rs] * (double)rows[(size_t)j * a.nk + jb];
           } else {
             const int32_t pa = __ldg(&a.as_pair[g0 + j]);
             const double g = __ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
-            sum += (pa > 0 ? g : -g) * (double)__ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + jb]);
+            sum += (pa > 0 ? g : -g) *
+                   (double)__ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + __ldg(&a.kets[jb])]);
           }
         }
         acc += pb > 0 ? sum : -sum;
@@ -536,10 +541,21 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
       if (bo[i + 1] > bo[i]) colp.push_back(make_uint2((uint32_t)i, bo[i]));
     const size_t ncs = colp.size();
     colp.push_back(make_uint2(0u, (uint32_t)nnz));
-    for (size_t f = 0; f < nnz; f++) bsp[f] = make_uint2(bket[f], (uint32_t)bpair[f]);
+    // the distinct kets of the beta singles, and each entry's ket as its position among them
+    std::vector<uint32_t> kets(bket.begin(), bket.begin() + nnz);
+    std::sort(kets.begin(), kets.end());
+    kets.erase(std::unique(kets.begin(), kets.end()), kets.end());
+    for (size_t f = 0; f < nnz; f++) {
+      const uint32_t pos = (uint32_t)(std::lower_bound(kets.begin(), kets.end(), bket[f]) - kets.begin());
+      bsp[f] = make_uint2(pos, (uint32_t)bpair[f]);
+    }
+    if (kets.empty()) kets.push_back(0);
     TPB_CUDA(cudaMalloc(&h->d_ab_rows, sizeof(uint32_t) * std::max<size_t>(1, rows.size())));
     TPB_CUDA(cudaMalloc(&h->d_ab_colp, sizeof(uint2) * colp.size()));
     TPB_CUDA(cudaMalloc(&h->d_ab_bsp, sizeof(uint2) * bsp.size()));
+    TPB_CUDA(cudaMalloc(&h->d_ab_kets, sizeof(uint32_t) * kets.size()));
+    TPB_CUDA(cudaMemcpy(h->d_ab_kets, kets.data(), sizeof(uint32_t) * kets.size(), cudaMemcpyHostToDevice));
+    h->ab_nkets = nnz ? (uint32_t)kets.size() : 0;
     if (!rows.empty())
       TPB_CUDA(cudaMemcpy(h->d_ab_rows, rows.data(), sizeof(uint32_t) * rows.size(), cudaMemcpyHostToDevice));
     TPB_CUDA(cudaMemcpy(h->d_ab_colp, colp.data(), sizeof(uint2) * colp.size(), cudaMemcpyHostToDevice));
@@ -558,6 +574,8 @@ int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
   a.rows = h->d_ab_rows;
   a.colp = h->d_ab_colp;
   a.bsp = h->d_ab_bsp;
+  a.kets = h->d_ab_kets;
+  a.nk = h->ab_nkets;
   a.ncols_s = h->ab_ncols;
   a.as_off = h->ta_s.off;
   a.as_ket = h->ta_s.ket;
@@ -565,9 +583,9 @@ int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
   a.eri = h->d_eri;
   a.L2 = h->L * h->L;
   a.nb = (uint32_t)h->bstr.size();
-  // one staged single = its C row and its integral row; aim for 4 CTAs per SM, else as many
-  // singles as fit in one CTA's shared memory
-  const size_t per = ((size_t)a.nb + a.L2) * sizeof(T);
+  // one staged single = its compacted C row and its integral row; aim for 4 CTAs per SM, else as
+  // many singles as fit in one CTA's shared memory
+  const size_t per = ((size_t)a.nk + a.L2) * sizeof(T);
   const size_t target = std::max<size_t>(per, h->smem_optin / 4 - 1024);
   if (per <= h->smem_optin) {
     a.group = (uint32_t)std::max<size_t>(1, std::min<size_t>(target / per, h->ab_max_k));

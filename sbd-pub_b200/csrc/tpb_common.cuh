@@ -175,7 +175,9 @@ struct sbd_tpb_handle {
   // sparse alpha-beta term: alpha rows and beta columns that have at least one single
   uint32_t *d_ab_rows = nullptr;
   uint2 *d_ab_colp = nullptr;  // per beta column with singles: (column, first entry); last: (0, nnz)
-  uint2 *d_ab_bsp = nullptr;   // beta singles entries packed as (ket, signed pair label)
+  uint2 *d_ab_bsp = nullptr;   // beta singles entries packed as (ket position in d_ab_kets, signed pair label)
+  uint32_t *d_ab_kets = nullptr;  // distinct kets of the beta singles, ascending
+  uint32_t ab_nkets = 0;
   uint32_t ab_nrows = 0, ab_ncols = 0, ab_max_k = 0;  // ab_max_k: most singles of one alpha row
   // learned preconditioner attached by sbd_tpb_set_preconditioner (not owned) and the
   // occupation windows of the strings it reads
