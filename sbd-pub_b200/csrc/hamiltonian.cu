@@ -118,6 +118,8 @@ __global__ void double_values_kernel(const uint64_t *__restrict__ str, uint32_t 
 }
 
 void free_prog(SigmaProg &p) {
+  free_dev(p.jtab);
+  free_dev(p.pmap);
   free_dev(p.s_val);
   free_dev(p.s_valf);
   free_dev(p.s_pair);
@@ -147,7 +149,49 @@ int build_prog(sbd_tpb_handle *h, const uint64_t *d_str, uint32_t n, const ExTab
   return SBD_TPB_OK;
 }
 
+// J[i][c] = sum over the orbitals k of col_str[c], ascending, of vd[pair(i)][k]
+__global__ void coulomb_table_kernel(const uint64_t *__restrict__ col_str, size_t ncols,
+                                     const int32_t *__restrict__ pairs, uint32_t npair, int L,
+                                     const double *__restrict__ vd, double *__restrict__ J) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)npair * ncols) return;
+  const uint32_t i = (uint32_t)(t / ncols);
+  const size_t c = t - (size_t)i * ncols;
+  const double *vrow = vd + (size_t)pairs[i] * L;
+  double o = 0.0;
+  for (uint64_t m = col_str[c]; m; m &= m - 1) o += __ldg(&vrow[lowest_bit(m)]);
+  J[t] = o;
+}
+
 }  // namespace
+
+int build_coulomb_table(sbd_tpb_handle *h, SigmaProg &p, const uint64_t *col_str, size_t ncols) {
+  if (p.jtab || !p.s || p.s->nnz == 0) return SBD_TPB_OK;
+  const int L2 = h->L * h->L;
+  std::vector<int32_t> sp(p.s->nnz), pmap(L2, -1), pairs;
+  TPB_CUDA(cudaMemcpy(sp.data(), p.s_pair, sizeof(int32_t) * sp.size(), cudaMemcpyDeviceToHost));
+  for (int32_t ps : sp) {
+    const int pr = (ps > 0 ? ps : -ps) - 1;
+    if (pmap[pr] < 0) {
+      pmap[pr] = (int32_t)pairs.size();
+      pairs.push_back(pr);
+    }
+  }
+  int32_t *d_pairs = nullptr;
+  TPB_CUDA(cudaMalloc(&p.pmap, sizeof(int32_t) * L2));
+  TPB_CUDA(cudaMalloc(&d_pairs, sizeof(int32_t) * pairs.size()));
+  TPB_CUDA(cudaMalloc(&p.jtab, sizeof(double) * pairs.size() * ncols));
+  TPB_CUDA(cudaMemcpy(p.pmap, pmap.data(), sizeof(int32_t) * L2, cudaMemcpyHostToDevice));
+  TPB_CUDA(cudaMemcpy(d_pairs, pairs.data(), sizeof(int32_t) * pairs.size(), cudaMemcpyHostToDevice));
+  p.npair = (uint32_t)pairs.size();
+  const size_t tot = pairs.size() * ncols;
+  coulomb_table_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(col_str, ncols, d_pairs, p.npair,
+                                                                             h->L, h->d_vd, p.jtab);
+  TPB_LAUNCHED(h);
+  TPB_CUDA(cudaStreamSynchronize(h->stream));
+  cudaFree(d_pairs);
+  return SBD_TPB_OK;
+}
 
 void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->d_eri);

@@ -105,6 +105,8 @@ struct BlockArgs {
   const double *d_val;
   const float *d_valf;
   const uint64_t *col_str;  // strings of the column spin (other-spin Coulomb term of singles)
+  const double *jtab;       // per-pair Coulomb sums over those strings (SigmaProg::jtab), or null
+  const int32_t *pmap;      // pair -> row of jtab
   const double *vd;         // (pq|kk) [L*L][L]
   int L;
   uint32_t nrows, ncols;    // X is nrows x ncols, row-major
@@ -225,15 +227,20 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       const double sg = ps > 0 ? 1.0 : -1.0;
       const double *vrow = a.vd + (size_t)pr * L;
       const T *xr = X + (size_t)ket * ncols;
+      const double *jr = a.jtab ? a.jtab + (size_t)__ldg(&a.pmap[pr]) * ncols : nullptr;
 #pragma unroll
       for (int i = 0; i < VW; i++) {
         if (!ok[i]) continue;
         const uint32_t c = cbase + i;
-        uint64_t occ = cstr[i];
         double o = 0.0;
-        while (occ) {
-          o += __ldg(&vrow[lowest_bit(occ)]);
-          occ &= occ - 1;
+        if (jr) {
+          o = __ldg(&jr[c]);
+        } else {
+          uint64_t occ = cstr[i];
+          while (occ) {
+            o += __ldg(&vrow[lowest_bit(occ)]);
+            occ &= occ - 1;
+          }
         }
         double x = (v + sg * o) * (double)__ldg(&xr[c]);
         if (kAlpha && a.do_ab) {
@@ -618,6 +625,9 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   }
   T *CT = reinterpret_cast<T *>(h->d_ct);
   TPB_CHECK(prepare_sigma_meta(h, !dense_ab));
+  // per-pair Coulomb sums of the singles over the other spin's strings (built once per problem)
+  TPB_CHECK(build_coulomb_table(h, h->pa, h->d_bstr, nb));
+  TPB_CHECK(build_coulomb_table(h, h->pb, h->d_astr, na));
 
   BlockArgs ba{};
   ba.s_off = h->ta_s.off;
@@ -630,6 +640,8 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   ba.d_val = h->pa.d_val;
   ba.d_valf = h->pa.d_valf;
   ba.col_str = h->d_bstr;
+  ba.jtab = h->pa.jtab;
+  ba.pmap = h->pa.pmap;
   ba.vd = h->d_vd;
   ba.L = h->L;
   ba.nrows = na;
@@ -660,6 +672,8 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   bb.d_val = h->pb.d_val;
   bb.d_valf = h->pb.d_valf;
   bb.col_str = h->d_astr;
+  bb.jtab = h->pb.jtab;
+  bb.pmap = h->pb.pmap;
   bb.vd = h->d_vd;
   bb.L = h->L;
   bb.nrows = nb;

@@ -95,6 +95,12 @@ struct SigmaProg {
   int32_t *s_pair = nullptr;
   double *d_val = nullptr;
   float *d_valf = nullptr;
+  // other-spin Coulomb sums of the singles: jtab[pidx(pq)][c] = sum_{k in string c of the column
+  // spin} (pq|kk), one row per pair pq that some single of this program carries (pmap[pq] = its
+  // row, -1 for the others); built by build_coulomb_table
+  double *jtab = nullptr;
+  int32_t *pmap = nullptr;
+  uint32_t npair = 0;
 };
 
 // Dense-path data for the alpha-beta term as gather -> (pq|rs) contraction -> scatter.
@@ -203,6 +209,8 @@ int copy_table_reference_layout(sbd_tpb_handle *h, int kind, uint64_t *off, uint
 int upload_hamiltonian(sbd_tpb_handle *h);
 int build_string_data(sbd_tpb_handle *h);
 int build_sigma_programs(sbd_tpb_handle *h);
+// jtab/pmap of a sigma program whose columns are the strings col_str[0..ncols)
+int build_coulomb_table(sbd_tpb_handle *h, SigmaProg &p, const uint64_t *col_str, size_t ncols);
 int compute_diagonal(sbd_tpb_handle *h);
 void free_device_problem(sbd_tpb_handle *h);
 // sigma.cu
