@@ -27,17 +27,16 @@ constexpr int kBlkRows = 8;  // bra rows per CTA
 constexpr int kBlkThreads = 128;
 // Thread mapping of a CTA per element type and pass: the 128 threads form G row groups, each
 // thread holding kBlkRows / G rows of VW columns (fewer accumulators per thread for larger G, so
-// more CTAs fit an SM), with the register budget of M CTAs per SM.  Measured at 4e8 determinants
-// (norb=32), ms per pass: FP32 alpha 1 group / 5 CTAs 6.38 (2/7: 6.47, 2/8 and 2/9 spill: 6.40;
-// 1/6: 6.42), FP32 beta 2/9 4.74 (1/5: 5.64, 2/7: 5.44, 2/8: 4.91, 2/10: 5.20), FP64 alpha 2/7
-// 8.36 (1/5: 10.23), FP64 beta 2/9 7.14 (1/5: 8.80, 2/8: 7.56).  Four groups lose the 16-byte runs
-// of the FP32 transposed write-out and run slower.  On large problems the FP32 alpha pass keeps one
-// group and parks the C values it writes out transposed in shared memory instead of 32 registers
-// (OS), which fits 7 CTAs per SM: 5.83 ms (registers, 5 CTAs: 6.36; parked, 5 or 6 CTAs: 6.49 /
-// 6.03; 8 CTAs spills: 6.56); parking gains nothing in FP64 (2/8: 8.17 at norb=32 but 4.20
-// against 3.83 at norb=28).  Its 512-column slabs leave small problems with too few CTAs (norb=12
-// FCI, 924 x 924: 0.84 ms against 0.48 with 2/7; 4,000 x 4,000: 1.31 against 1.16), so below
-// 10,000 CTAs it takes 2/7.
+// more CTAs fit an SM), with the register budget of M CTAs per SM; OS parks the C values the alpha
+// pass writes out transposed in shared memory instead of registers.  Measured at 4e8 determinants
+// (norb=32), ms per pass, with the singles' Coulomb sums from the per-pair table: FP32 alpha 2/8/OS
+// 4.33 (1/7/OS: 4.71, 1/8/OS: 5.11, 2/9: 5.08, 2/9/OS and 2/10/OS spill: 4.67 / 5.60), FP32 beta
+// 2/9 3.61 (2/10: 3.71), FP64 alpha 2/7 6.62 (2/9: 6.87), FP64 beta 2/9 5.91 (2/10: 6.41).  Before
+// the table the loop over the column string's orbitals set other optima (FP32 alpha 1/7/OS, 6.36
+// -> 5.83 ms with parking).  Four groups lose the 16-byte runs of the FP32 transposed write-out.
+// Small problems run the FP32 alpha pass with 2/7 and no parking (norb=12 FCI 0.22 ms against
+// 0.26 with 2/8/OS; 4,000 x 4,000: 0.60 against 0.62; one-group slabs of 512 columns were worse
+// still there: 0.84 / 1.31 before the table); the switch is at 10,000 one-group CTAs.
 // The mapping of a pass as template arguments: G row groups, register budget of M CTAs per SM.
 template <typename T>
 __device__ __forceinline__ T val_of(const double *v, const float *vf, uint32_t e);
@@ -492,7 +491,7 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   if constexpr (sizeof(T) == 4 && kAlpha) {
     const size_t blocks_g1 =
         ((ba.nrows + kBlkRows - 1) / kBlkRows) * ((ba.ncols + kBlkThreads * 4 - 1) / (kBlkThreads * 4));
-    if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 1, 7, true>(h, ba, X, out, XT);
+    if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 2, 8, true>(h, ba, X, out, XT);
     return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
   } else if constexpr (kAlpha) {
     return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
