@@ -166,7 +166,8 @@ __global__ void coulomb_table_kernel(const uint64_t *__restrict__ col_str, size_
 }  // namespace
 
 int build_coulomb_table(sbd_tpb_handle *h, SigmaProg &p, const uint64_t *col_str, size_t ncols) {
-  if (p.jtab || !p.s || p.s->nnz == 0) return SBD_TPB_OK;
+  if (p.jtab_tried || !p.s || p.s->nnz == 0) return SBD_TPB_OK;
+  p.jtab_tried = true;
   const int L2 = h->L * h->L;
   std::vector<int32_t> sp(p.s->nnz), pmap(L2, -1), pairs;
   TPB_CUDA(cudaMemcpy(sp.data(), p.s_pair, sizeof(int32_t) * sp.size(), cudaMemcpyDeviceToHost));
@@ -177,10 +178,22 @@ int build_coulomb_table(sbd_tpb_handle *h, SigmaProg &p, const uint64_t *col_str
       pairs.push_back(pr);
     }
   }
+  // the table is an optimisation: above 1/16 of the free device memory (or if it cannot be
+  // allocated) the singles keep the loop over the column string's orbitals
+  const size_t bytes = sizeof(double) * pairs.size() * ncols;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || bytes > free_b / 16) {
+    cudaGetLastError();
+    return SBD_TPB_OK;
+  }
+  if (cudaMalloc(&p.jtab, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    p.jtab = nullptr;
+    return SBD_TPB_OK;
+  }
   int32_t *d_pairs = nullptr;
   TPB_CUDA(cudaMalloc(&p.pmap, sizeof(int32_t) * L2));
   TPB_CUDA(cudaMalloc(&d_pairs, sizeof(int32_t) * pairs.size()));
-  TPB_CUDA(cudaMalloc(&p.jtab, sizeof(double) * pairs.size() * ncols));
   TPB_CUDA(cudaMemcpy(p.pmap, pmap.data(), sizeof(int32_t) * L2, cudaMemcpyHostToDevice));
   TPB_CUDA(cudaMemcpy(d_pairs, pairs.data(), sizeof(int32_t) * pairs.size(), cudaMemcpyHostToDevice));
   p.npair = (uint32_t)pairs.size();

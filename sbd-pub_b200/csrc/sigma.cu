@@ -105,6 +105,7 @@ struct BlockArgs {
   const float *d_valf;
   const uint64_t *col_str;  // strings of the column spin (other-spin Coulomb term of singles)
   const double *jtab;       // per-pair Coulomb sums over those strings (SigmaProg::jtab), or null
+                            // (then the singles loop over the column string's orbitals)
   const int32_t *pmap;      // pair -> row of jtab
   const double *vd;         // (pq|kk) [L*L][L]
   int L;

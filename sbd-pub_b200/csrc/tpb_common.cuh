@@ -101,6 +101,7 @@ struct SigmaProg {
   double *jtab = nullptr;
   int32_t *pmap = nullptr;
   uint32_t npair = 0;
+  bool jtab_tried = false;  // built, or found too large, once per program
 };
 
 // Dense-path data for the alpha-beta term as gather -> (pq|rs) contraction -> scatter.
