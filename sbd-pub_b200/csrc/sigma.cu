@@ -228,6 +228,22 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       const double *vrow = a.vd + (size_t)pr * L;
       const T *xr = X + (size_t)ket * ncols;
       const double *jr = a.jtab ? a.jtab + (size_t)__ldg(&a.pmap[pr]) * ncols : nullptr;
+      if (kVec && full && jr && !a.do_ab) {
+        // whole 16-byte column group: the ket values and the table's Coulomb sums as vector
+        // loads (table rows are ncols doubles, ncols a multiple of VW, so jr + cbase is aligned)
+        Vec<T, VW, true> xv;
+        xv.load(xr + cbase);
+        double o[VW];
+#pragma unroll
+        for (int i = 0; i < VW; i += 2) {
+          const double2 jj = __ldg(reinterpret_cast<const double2 *>(jr + cbase + i));
+          o[i] = jj.x;
+          o[i + 1] = jj.y;
+        }
+#pragma unroll
+        for (int i = 0; i < VW; i++) acc[r][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+        continue;
+      }
 #pragma unroll
       for (int i = 0; i < VW; i++) {
         if (!ok[i]) continue;
