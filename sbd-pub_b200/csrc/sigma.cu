@@ -28,15 +28,15 @@ constexpr int kBlkThreads = 128;
 // Thread mapping of a CTA per element type and pass: the 128 threads form G row groups, each
 // thread holding kBlkRows / G rows of VW columns (fewer accumulators per thread for larger G, so
 // more CTAs fit an SM), with the register budget of M CTAs per SM; OS parks the C values the alpha
-// pass writes out transposed in shared memory instead of registers.  Measured at 4e8 determinants
-// (norb=32), ms per pass, with the singles' Coulomb sums from the per-pair table: FP32 alpha 2/8/OS
-// 4.33 (1/7/OS: 4.71, 1/8/OS: 5.11, 2/9: 5.08, 2/9/OS and 2/10/OS spill: 4.67 / 5.60), FP32 beta
-// 2/9 3.61 (2/10: 3.71), FP64 alpha 2/7 6.62 (2/9: 6.87), FP64 beta 2/9 5.91 (2/10: 6.41).  Before
-// the table the loop over the column string's orbitals set other optima (FP32 alpha 1/7/OS, 6.36
-// -> 5.83 ms with parking).  Four groups lose the 16-byte runs of the FP32 transposed write-out.
-// Small problems run the FP32 alpha pass with 2/7 and no parking (norb=12 FCI 0.22 ms against
-// 0.26 with 2/8/OS; 4,000 x 4,000: 0.60 against 0.62; one-group slabs of 512 columns were worse
-// still there: 0.84 / 1.31 before the table); the switch is at 10,000 one-group CTAs.
+// pass writes out transposed in shared memory instead of registers.  Measured with the singles'
+// Coulomb sums read from the per-pair table as 16-byte loads, ms per pass at 4e8 determinants
+// (norb=32) / 1e8 (norb=28) / norb=12 FCI: FP32 alpha 2/8/OS 3.31 / 1.45 (2/7: 3.59 / 1.48,
+// 2/8: 3.66 / 1.52, 1/6/OS: 3.77 / 1.50, 2/9/OS spills: 3.84 / 1.78); FP32 beta 2/8 3.35 / 1.36 /
+// 0.159 (2/9: 3.38 / 1.44 / 0.185, 2/10: 3.68 / 1.63, 4/10: 14.4); FP64 alpha 2/7 6.39 / 2.53 /
+// 0.187 (2/8: 6.44, 2/7/OS: 6.45, 2/6: 6.95); FP64 beta 2/9 5.76 / 2.71 / 0.196 (2/8: 5.93 / 2.38 /
+// 0.197, 2/10: 6.09).  Four groups lose the 16-byte runs of the FP32 transposed write-out.  Small
+// problems run the FP32 alpha pass with 2/6 and no parking (norb=12 FCI 0.154 ms; 2/7: 0.159,
+// 2/7/OS: 0.161, 2/8/OS: 0.170, 1/5: 0.279); the switch is at 10,000 one-group CTAs.
 // The mapping of a pass as template arguments: G row groups, register budget of M CTAs per SM.
 template <typename T>
 __device__ __forceinline__ T val_of(const double *v, const float *vf, uint32_t e);
@@ -509,9 +509,11 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
     const size_t blocks_g1 =
         ((ba.nrows + kBlkRows - 1) / kBlkRows) * ((ba.ncols + kBlkThreads * 4 - 1) / (kBlkThreads * 4));
     if (blocks_g1 >= 10000) return launch_block_cfg<T, kAlpha, 2, 8, true>(h, ba, X, out, XT);
-    return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
+    return launch_block_cfg<T, kAlpha, 2, 6>(h, ba, X, out, XT);
   } else if constexpr (kAlpha) {
     return launch_block_cfg<T, kAlpha, 2, 7>(h, ba, X, out, XT);
+  } else if constexpr (sizeof(T) == 4) {
+    return launch_block_cfg<T, kAlpha, 2, 8>(h, ba, X, out, XT);
   } else {
     return launch_block_cfg<T, kAlpha, 2, 9>(h, ba, X, out, XT);
   }
