@@ -181,7 +181,7 @@ struct sbd_tpb_handle {
   size_t ab_work_bytes = 0;
   // sparse alpha-beta term: alpha rows and beta columns that have at least one single
   uint32_t *d_ab_rows = nullptr;
-  uint2 *d_ab_colp = nullptr;  // per beta column with singles: (column, first entry); last: (0, nnz)
+  uint2 *d_ab_colp = nullptr;  // per beta column with singles, most singles first: (column, first entry); last: (0, nnz)
   uint2 *d_ab_bsp = nullptr;   // beta singles entries packed as (ket position in d_ab_kets, signed pair label)
   uint32_t *d_ab_kets = nullptr;  // distinct kets of the beta singles, ascending
   uint32_t ab_nkets = 0;
