@@ -468,7 +468,7 @@ def run_ours(args, world, rank, local, pg):
     achieved = per[dom] / (kern[dom] * 1e-3) / 1e9
     # DRAM bytes per determinant of each pass from the ncu capture at 10^8 determinants (FP32,
     # profiles/sigma_kernels_sci28_fp32.md), scaled to this workload's determinants
-    traffic_per_det = {"sigma_block_kernel<alpha>": 18.27, "sigma_block_kernel<beta>": 12.93}
+    traffic_per_det = {"sigma_block_kernel<alpha>": 17.69, "sigma_block_kernel<beta>": 12.60}
     traffic = (traffic_per_det[names[dom]] * N / 1e9
                if dt == torch.float32 and names[dom] in traffic_per_det else None)
     roofline = {"kernel": names[dom], "bound": "hbm", "achieved": achieved,
