@@ -368,17 +368,23 @@ def time_to_solution(h, args):
     import sbd_tpb
     out = {}
 
-    def solve(name, **kw):
+    def solve(name, runs=2, **kw):
+        # each compared solve runs twice and the faster wall time is reported (both are listed):
+        # a step synchronises with the host two or three times, and on a host shared with other
+        # jobs single solves were seen up to 40 % slower than the same solve run again
         p = sbd_tpb.default_params(max_it=40, max_nb=8, **kw)
-        torch.cuda.synchronize()
-        ts = time.perf_counter()
-        r = h.davidson(p, want_vector=False)
-        out[name] = {"seconds": time.perf_counter() - ts, "sigma_steps": r["iterations"],
+        times = []
+        for _ in range(runs):
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            r = h.davidson(p, want_vector=False)
+            times.append(time.perf_counter() - ts)
+        out[name] = {"seconds": min(times), "seconds_runs": times, "sigma_steps": r["iterations"],
                      "energy": r["energy"], "residual": r["residual"], "converged": r["converged"],
                      "eps": kw.get("eps"), "learned_steps": r["learned_steps"],
                      "fallback_steps": r["fallback_steps"]}
 
-    solve("fp64_reference", eps=1e-6, precision=sbd_tpb.FP64)
+    solve("fp64_reference", runs=1, eps=1e-6, precision=sbd_tpb.FP64)
     solve("fp64", eps=1e-4, precision=sbd_tpb.FP64)
     solve("mixed", eps=1e-4, precision=sbd_tpb.MIXED)
     pc, train = train_preconditioner(h.device)
@@ -393,7 +399,8 @@ def time_to_solution(h, args):
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["speedup_mixed_learned_vs_fp64"] = out["fp64"]["seconds"] / out["mixed_learned"]["seconds"]
     out["note"] = ("training (pairs from the 12- and 24-orbital problems) is timed separately and not "
-                   "part of the solve times")
+                   "part of the solve times; seconds = the faster of seconds_runs (two runs of each "
+                   "compared solve)")
     return out
 
 
