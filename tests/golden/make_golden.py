@@ -202,14 +202,50 @@ def make_strings_fixture(out_dir):
     return meta
 
 
+# Larger selected sets of the reference's data directories with the energies its READMEs publish
+# (8 decimals).  The Hamiltonians are those of the h2o_1em3 / n2_1em3 fixtures (same FCIDUMP).
+PUBLISHED = {
+    "h2o_1em4": ("h2o_1em3", "data/h2o/h2o-1em4-alpha.txt", -76.24295848, "data/h2o/README.md:7"),
+    "h2o_1em5": ("h2o_1em3", "data/h2o/h2o-1em5-alpha.txt", -76.24373504, "data/h2o/README.md:8"),
+    "h2o_1em6": ("h2o_1em3", "data/h2o/h2o-1em6-alpha.txt", -76.24377593, "data/h2o/README.md:9"),
+    "h2o_1em7": ("h2o_1em3", "data/h2o/h2o-1em7-alpha.txt", -76.24377678, "data/h2o/README.md:10"),
+    "n2_3em4": ("n2_1em3", "data/n2/3em4-alpha.txt", -109.04697304, "data/n2/README.md:7"),
+    "n2_1em4": ("n2_1em3", "data/n2/1em4-alpha.txt", -109.04835269, "data/n2/README.md:8"),
+    "n2_1em5": ("n2_1em3", "data/n2/1em5-alpha.txt", -109.04871934, "data/n2/README.md:10"),
+    "n2_1em6": ("n2_1em3", "data/n2/1em6-alpha.txt", -109.04874139, "data/n2/README.md:12"),
+}
+
+
+def make_published_fixture(out_dir):
+    """tests/golden/published.npz: the string sets of PUBLISHED, read by the oracle's LoadAlphaDets
+    restatement (orc_load_strings, held equal to the reference's reader by tests/test_strings.py),
+    and their published energies in the index."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    data, meta = {}, {}
+    for name, (base, adet, energy, src) in PUBLISHED.items():
+        L = json.load(open(os.path.join(HERE, "cases.json")))[base]["norb"]
+        a = pyoracle.load_strings(os.path.join(REF, adet), L)
+        data[f"{name}_astr"] = a
+        meta[name] = dict(base=base, adet=adet, published=energy, published_src=src, na=int(len(a)),
+                          ndet=int(len(a)) ** 2)
+    np.savez_compressed(os.path.join(out_dir, "published.npz"), **data)
+    return meta
+
+
 def main():
-    names = sys.argv[1:] or list(CASES) + ["strings"]
+    names = sys.argv[1:] or list(CASES) + ["strings", "published"]
     index_path = os.path.join(HERE, "cases.json")
     index = json.load(open(index_path)) if os.path.exists(index_path) else {}
     if "strings" in names:
         names = [n for n in names if n != "strings"]
         print("case strings", flush=True)
         index["strings"] = make_strings_fixture(HERE)
+        json.dump(index, open(index_path, "w"), indent=1, sort_keys=True)
+    if "published" in names:
+        names = [n for n in names if n != "published"]
+        print("case published", flush=True)
+        index["published"] = make_published_fixture(HERE)
         json.dump(index, open(index_path, "w"), indent=1, sort_keys=True)
     for name in names:
         print("case", name, flush=True)
