@@ -1,6 +1,7 @@
 """The drop-in CLI (sbd-pub_b200/bin/diag) with the reference app's flags, run on FCIDUMP and
 string files written from the n2 fixture: the energy line matches the reference's energy and the
-RDM files and energy decomposition are produced (GPU)."""
+RDM files and energy decomposition are produced (GPU).  On the CPU: its flag checks, FCIDUMP errors
+and the error it stops with when there is no device."""
 import os
 import re
 import subprocess
@@ -17,6 +18,65 @@ def test_cli_binary_built_and_rejects_bad_flags(tmp_path):
     assert os.path.exists(DIAG), "build with make -C sbd-pub_b200"
     r = subprocess.run([DIAG, "--method", "3"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
+
+
+# Host-side checks that run before any device call: flag values the drop-in does not build (the
+# reference app accepts them, main.cc) and malformed FCIDUMP files (fcidump.h:29-141 reads them)
+BAD_FLAGS = [
+    (["--method", "1"], "only the matrix-free solvers are built"),
+    (["--method", "3"], "only the matrix-free solvers are built"),
+    (["--bit_length", "0"], "--bit_length must be in [1, 64]"),
+    (["--bit_length", "65"], "--bit_length must be in [1, 64]"),
+    (["--adet_comm_size", "2"], "one rank on one GPU: --*_comm_size must be 1"),
+    (["--task_comm_size", "4"], "one rank on one GPU: --*_comm_size must be 1"),
+    (["--init", "1"], "only --init 0"),
+    (["--carryover_type", "4"], "--carryover_type must be 0, 1, 2 or 3"),
+    (["--precision", "fp16"], "--precision must be fp64 or mixed"),
+    (["--preconditioner", "jacobi"], "--preconditioner must be diagonal or learned"),
+    (["--dump_matrix_form_wf", "wf.txt"], "not built in this version: --dump_matrix_form_wf"),
+    (["--tolerance"], "missing value for --tolerance"),
+]
+
+
+@pytest.mark.parametrize("args,msg", BAD_FLAGS)
+def test_cli_flag_errors(args, msg, tmp_path):
+    r = subprocess.run([DIAG] + args, capture_output=True, text=True, timeout=60, cwd=str(tmp_path))
+    assert r.returncode == 1
+    assert r.stderr.startswith("diag: ") and msg in r.stderr
+
+
+FCIDUMPS = {
+    "no_norb": (" &FCI NELEC=2,MS2=0,\n &END\n 0.5 1 1 1 1\n", "FCIDUMP header has no NORB"),
+    "norb_65": (" &FCI NORB=65,NELEC=2,\n &END\n 0.5 1 1 1 1\n", "NORB must be in [1, 64]"),
+    "one_body_index": (" &FCI NORB=2,NELEC=2,\n &END\n -1.0 3 1 0 0\n", "one-electron index out of range"),
+    "two_body_index": (" &FCI NORB=2,NELEC=2,\n &END\n 0.5 1 1 2 3\n", "two-electron index out of range"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(FCIDUMPS))
+def test_cli_fcidump_errors(case, tmp_path):
+    text, msg = FCIDUMPS[case]
+    (tmp_path / "fcidump.txt").write_text(text)
+    r = subprocess.run([DIAG, "--fcidump", str(tmp_path / "fcidump.txt")], capture_output=True, text=True,
+                       timeout=60, cwd=str(tmp_path))
+    assert r.returncode == 1 and msg in r.stderr
+    r = subprocess.run([DIAG, "--fcidump", str(tmp_path / "missing.txt")], capture_output=True, text=True,
+                       timeout=60, cwd=str(tmp_path))
+    assert r.returncode == 1 and "Failed to open FCIDUMP file" in r.stderr
+
+
+def test_cli_fails_loudly_without_a_device(tmp_path):
+    """A valid input on a machine without a GPU: the CLI stops with the library's error (there is
+    no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    (tmp_path / "fcidump.txt").write_text(" &FCI NORB=2,NELEC=2,MS2=0,\n &END\n 0.5 1 1 1 1\n -1.0 1 1 0 0\n"
+                                          " -0.5 2 2 0 0\n 0.1 0 0 0 0\n")
+    (tmp_path / "a.txt").write_text("01\n10\n")
+    r = subprocess.run([DIAG, "--fcidump", "fcidump.txt", "--adetfile", "a.txt"], capture_output=True, text=True,
+                       timeout=60, cwd=str(tmp_path))
+    assert r.returncode == 1 and r.stderr.strip() == "diag: no CUDA device"
 
 
 @pytest.mark.gpu
