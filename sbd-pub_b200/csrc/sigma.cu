@@ -130,9 +130,12 @@ struct BlockArgs {
 // slab-major so the CTAs in flight gather from one slab of X that stays in L2.  The block's table
 // entries (one contiguous CSR range) are staged in shared memory first, so the gathers
 // X[ket, cols] issue back to back.
-//   alpha pass (kAlpha): X = C.  Adds the diagonal and the alpha-single x beta-single terms and
-//     writes sigma[Ia, Ib] once; the thread's own C[Ia-block, cols] values go out transposed to
-//     C^T as contiguous runs of its rows.
+//   alpha pass (kAlpha): X = C.  Adds the diagonal (and, in the allocation-free path only, the
+//     alpha-single x beta-single terms, which otherwise have kernels of their own) and writes
+//     sigma[Ia, Ib] once; the thread's own C[Ia-block, cols] values go out transposed to C^T as
+//     contiguous runs of its rows.  Singles read the other spin's Coulomb sums from the per-pair
+//     table when it exists (16-byte loads for a whole column group), else loop over the column
+//     string's orbitals.
 //   beta pass: X = C^T.  Each thread adds its rows x VW results into sigma[Ia, Ib0 ...)
 //     (contiguous along Ib) for its columns Ia.
 template <typename T, bool kAlpha, bool kVec, int G, int M, bool OS>
