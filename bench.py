@@ -1,22 +1,29 @@
 """Benchmark of the TPB sigma hot path on B200 (one JSON line on rank 0).
 
-A step is one sigma = H*C over the whole determinant space of the workload (default: norb=32,
-10+10 electrons, 20,000 x 20,000 strings = 400M determinants, seeded synthetic integrals and
-strings as the reference's molecular inputs would give them).  `value` is sigma GDets/s with the
-vectors resident in HBM (the library's internal sign convention, no conversion passes); `e2e`
-is the same through the reference-facing C ABI call sbd_tpb_sigma with host buffers (H2D of C,
-sign conversions, D2H of sigma inside the timed region).  Multi-GPU runs are replicas (the
-path has no data exchange on one node in this build): every rank solves its own copy and
-`value` is the aggregate.  `--impl reference` times the reference's own CPU sigma (compiled
-unchanged under oracle/_ref) on a bounded sample of the same workload with all host threads.
+A step is one sigma = H*C in FP64 (the reference's arithmetic) over the whole determant space of
+the workload (default: norb=32, 10+10 electrons, 20,000 x 20,000 strings = 400M determinants,
+seeded synthetic integrals and strings as the reference's molecular inputs would give them).
+`value` is sigma GDets/s with the vectors resident in HBM (the library's internal sign convention,
+no conversion passes); `e2e` is the same through the reference-facing C ABI call sbd_tpb_sigma
+with host buffers (H2D of C, sign conversions, D2H of sigma inside the timed region).  The FP32
+sigma of the mixed-precision path is reported beside it (`sigma_f32`).  Multi-GPU runs are
+replicas (the path has no data exchange on one node in this build): every rank solves its own
+copy and `value` is the aggregate.  `cpu_baseline` is the reference's own CPU sigma (compiled
+unchanged under oracle/_ref) on the whole problem, once, with all host threads; `--impl reference`
+times the same reference sigma per step on bra-row blocks of the whole problem (every connection
+of the block's rows), spread evenly over the alpha strings.
 
-The line also carries `strings` (a 2,000,000-line string file parsed, sorted and de-duplicated on
-the GPU, beside the reference's LoadAlphaDets on the host) and `carryover`: the carry-over string selection (sbd_tpb_carryover_strings,
-the step after the solve in the reference's sbd::tpb::diag) on an FP64 vector of the workload,
-with the roofline of its pass over W and the CPU restatement timed on a sample of rows.
+The line also carries `time_to_solution` (Davidson from the HF start: plain FP64 against mixed
+precision and mixed precision with the learned preconditioner, median of three solves each),
+`learned_cfg4` (the learned against the diagonal correction on the 28-orbital 100M-determinant
+problem), `strings` (a 2,000,000-line string file parsed, sorted and de-duplicated on the GPU,
+beside the reference's LoadAlphaDets on the host) and `carryover`: the carry-over string
+selection (sbd_tpb_carryover_strings, the step after the solve in the reference's
+sbd::tpb::diag) on an FP64 vector of the workload, with the roofline of its pass over W and the
+CPU restatement timed on a sample of rows.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload sci32]
-                    [--precision mixed|fp64] [--impl ours|reference] [--no-solve] [--no-carryover]
+                    [--precision fp64|mixed] [--impl ours|reference] [--no-solve] [--no-carryover]
 """
 from __future__ import annotations
 
@@ -37,6 +44,9 @@ sys.path.insert(0, os.path.join(ROOT, "sbd-pub_b200", "python"))
 
 METRIC = "sigma GDets/s; time to 1e-6 Ha: mixed+learned vs plain FP64, 1 B200"
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+# DRAM bytes per determinant of the FP64 passes (ncu, 10^8 determinants, norb=28)
+TRAFFIC_F64_ALPHA = None
+TRAFFIC_F64_BETA = None
 
 
 def parse():
@@ -45,11 +55,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="sci32")
-    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64",
+                    help="arithmetic of the headline sigma (the other one is reported beside it)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution solves")
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
+    ap.add_argument("--cpu-step-seconds", type=float, default=4.0,
+                    help="reference arm: host seconds of one step (a bra-row block of the problem)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sigma")
+    ap.add_argument("--no-cfg4", action="store_true",
+                    help="skip the learned-vs-diagonal solves on the 28-orbital problem")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
     ap.add_argument("--no-carryover", action="store_true", help="skip the carry-over measurement")
     ap.add_argument("--davidson-cycle", action="store_true",
@@ -158,37 +172,55 @@ def replica_throughput(pg, ms_local, dets_local, world, device="cpu"):
     return ms_max, world * dets_local / (ms_max * 1e-3) / 1e9
 
 
-def cpu_reference_sigma(prob_name, seconds_target, reps=1, threads=None):
-    """Time the reference's CPU sigma (oracle/_ref/ref_bench) on the first `amax` alpha strings x
-    all beta strings of the workload; amax is sized so the sample takes ~seconds_target."""
+def _ref_inputs(tmp, prob_name):
     import synth
-    if not os.path.exists(REF_BENCH):
-        return None
     L, n, cnt = synth.CONFIGS[prob_name]
     h1, eri, core = synth.synthetic_hamiltonian(L)
-    strs = synth.sample_strings(L, n, cnt)
-    env = dict(os.environ)
+    fd, fa = os.path.join(tmp, "fcidump.txt"), os.path.join(tmp, "a.txt")
+    synth.write_fcidump(fd, L, 2 * n, h1, eri, core)
+    synth.write_strings(fa, synth.sample_strings(L, n, cnt), L)
+    return fd, fa
+
+
+def _run_ref_bench(args_, threads):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    out = subprocess.run([REF_BENCH, *args_], capture_output=True, text=True, env=env, check=True).stdout
+    return dict(tok.split("=", 1) for tok in out.split())
+
+
+def cpu_reference_sigma_full(prob_name, threads=None):
+    """One call of the reference's CPU sigma (oracle/_ref/ref_bench: sbd::mult, tpb/mult.h:625-881)
+    over the whole problem -- every string, every connection -- with all host threads."""
+    if not os.path.exists(REF_BENCH):
+        return None
     threads = threads or os.cpu_count()
-    env["OMP_NUM_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory() as tmp:
-        fd, fa = os.path.join(tmp, "fcidump.txt"), os.path.join(tmp, "a.txt")
-        synth.write_fcidump(fd, L, 2 * n, h1, eri, core)
-        synth.write_strings(fa, strs, L)
+        fd, fa = _ref_inputs(tmp, prob_name)
+        kv = _run_ref_bench(["--fcidump", fd, "--adetfile", fa, "--reps", "1", "--no_hii"], threads)
+    return dict(ndet=int(kv["ndet"]), sigma_s=float(kv["sigma_s"].split(",")[0]),
+                helper_s=float(kv["helper_s"]), threads=int(kv["threads"]))
 
-        def run(amax, reps_):
-            out = subprocess.run([REF_BENCH, "--fcidump", fd, "--adetfile", fa, "--amax", str(amax),
-                                  "--reps", str(reps_)], capture_output=True, text=True, env=env,
-                                 check=True).stdout
-            kv = dict(tok.split("=", 1) for tok in out.split())
-            return int(kv["ndet"]), [float(x) for x in kv["sigma_s"].split(",")], float(kv["helper_s"])
 
-        amax = max(2, min(len(strs), 16))
-        ndet, ts, _ = run(amax, 1)
-        per_det = max(ts[0], 1e-4) / ndet
-        amax = int(min(len(strs), max(2, seconds_target / per_det / len(strs))))
-        ndet, ts, helper_s = run(amax, reps)
-    return dict(ndet=ndet, amax=amax, sigma_s=ts, helper_s=helper_s, threads=threads,
-                nstrings=len(strs))
+def cpu_reference_sigma_blocks(prob_name, blocks, target_s, threads=None):
+    """The reference's CPU sigma on `blocks` bra-row blocks of the whole problem (each block: its
+    alpha strings x all beta strings with all their connections, blocks spread evenly over the
+    sorted alpha list, rows per block sized for ~target_s seconds), after one call with an empty
+    bra range that measures mult's fixed N-sized work (ket copy, diagonal pass).  Per block, the
+    time charged is the block call minus the fixed part plus the block's share of it (rows/na)."""
+    if not os.path.exists(REF_BENCH):
+        return None
+    threads = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as tmp:
+        fd, fa = _ref_inputs(tmp, prob_name)
+        kv = _run_ref_bench(["--fcidump", fd, "--adetfile", fa, "--no_hii", "--blocks", str(blocks),
+                             "--target_s", repr(float(target_s))], threads)
+    na, nb, rows = int(kv["na"]), int(kv["nb"]), int(kv["rows"])
+    fixed = float(kv["fixed_s"])
+    raw = [float(x) for x in kv["block_s"].split(",")]
+    charged = [max(1e-9, t - fixed + fixed * rows / na) for t in raw]
+    return dict(na=na, nb=nb, rows=rows, fixed_s=fixed, block_s=raw, charged_s=charged,
+                block_start=[int(x) for x in kv["block_start"].split(",")],
+                threads=int(kv["threads"]), helper_s=float(kv["helper_s"]))
 
 
 def run_reference(args, world, rank):
@@ -200,22 +232,29 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built "
                           "(needs the reference checkout at build time)"}))
         return
-    per_step = max(1.0, args.cpu_sample_seconds / max(1, args.steps))
-    r = cpu_reference_sigma(args.workload, per_step, reps=args.warmup + args.steps)
-    ts = r["sigma_s"][args.warmup:]
+    r = cpu_reference_sigma_blocks(args.workload, args.warmup + args.steps, args.cpu_step_seconds)
+    ts = r["charged_s"][args.warmup:]
     t = sum(ts)
-    val = r["ndet"] * len(ts) / t / 1e9
-    sample = (f"first {r['amax']} of {r['nstrings']} alpha strings x all {r['nstrings']} beta "
-              f"strings ({r['ndet']} determinants) per step, reference sbd::mult (tpb/mult.h:625-881)")
+    dets = r["rows"] * r["nb"]
+    val = dets * len(ts) / t / 1e9
+    sample = (f"per step: {r['rows']} consecutive alpha strings x all {r['nb']} beta strings "
+              f"({dets} determinants) with every connection of the whole {r['na']} x {r['nb']} "
+              f"problem, one reference sbd::mult call (tpb/mult.h:625-881); {args.warmup + args.steps} "
+              f"blocks spread evenly over the sorted alpha strings (the first {args.warmup} are "
+              f"warm-up); mult's fixed N-sized pass ({r['fixed_s']:.3f} s: ket copy, diagonal) "
+              f"charged by the block's share of the rows")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": val, "unit": "GDets/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(ts),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"{args.workload}: norb={L}, {n}+{n} electrons, "
-                                        f"{cnt} x {cnt} strings", "sample": sample},
+        "data": "synthetic (seeded integrals 1729, strings 137)",
+        "config": {"workload": f"{args.workload}: norb={L}, {n}+{n} electrons, {cnt} x {cnt} strings",
+                   "determinants": r["na"] * r["nb"], "sample": sample},
         "cpu_baseline": {"value": val, "unit": "GDets/s", "cores": r["threads"], "kind": "reference",
                          "sample": sample},
         "e2e": {"value": val, "unit": "GDets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "blocks": {"rows": r["rows"], "block_start": r["block_start"], "block_s": r["block_s"],
+                   "fixed_s": r["fixed_s"], "helper_s": r["helper_s"]},
     }))
 
 
@@ -359,49 +398,120 @@ def strings_measure(h, args, cpu_sample=True):
     return out
 
 
-def time_to_solution(h, args):
+def _solve(h, params, runs=3):
+    """Wall times of `runs` whole Davidson solves with the same parameters; the median one is
+    reported, with every run's time and step count."""
+    import statistics as st
+
+    import torch
+    recs = []
+    for _ in range(runs):
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        r = h.davidson(params, want_vector=False)
+        recs.append((time.perf_counter() - ts, r))
+    times = [t for t, _ in recs]
+    med = st.median(times)
+    t, r = min(recs, key=lambda tr: abs(tr[0] - med))
+    return {"seconds": med, "seconds_runs": times, "sigma_steps": r["iterations"],
+            "sigma_steps_runs": [x["iterations"] for _, x in recs],
+            "energy": r["energy"], "residual": r["residual"], "converged": r["converged"],
+            "eps": params.eps, "learned_steps": r["learned_steps"], "fallback_steps": r["fallback_steps"]}
+
+
+def time_to_solution(h, args, pc):
     """Wall time of whole Davidson solves from the HF start: the FP64 reference answer (residual
     1e-6), then plain FP64, mixed precision and mixed precision + learned preconditioner, all to
-    residual 1e-4 (energy error ~ residual^2, far below 1e-6 Ha)."""
-    import torch
-
+    residual 1e-4 (energy error ~ residual^2, far below 1e-6 Ha), median of three solves each."""
     import sbd_tpb
     out = {}
-
-    def solve(name, runs=2, **kw):
-        # each compared solve runs twice and the faster wall time is reported (both are listed):
-        # a step synchronises with the host two or three times, and on a host shared with other
-        # jobs single solves were seen up to 40 % slower than the same solve run again
-        p = sbd_tpb.default_params(max_it=40, max_nb=8, **kw)
-        times = []
-        for _ in range(runs):
-            torch.cuda.synchronize()
-            ts = time.perf_counter()
-            r = h.davidson(p, want_vector=False)
-            times.append(time.perf_counter() - ts)
-        out[name] = {"seconds": min(times), "seconds_runs": times, "sigma_steps": r["iterations"],
-                     "energy": r["energy"], "residual": r["residual"], "converged": r["converged"],
-                     "eps": kw.get("eps"), "learned_steps": r["learned_steps"],
-                     "fallback_steps": r["fallback_steps"]}
-
-    solve("fp64_reference", runs=1, eps=1e-6, precision=sbd_tpb.FP64)
-    solve("fp64", eps=1e-4, precision=sbd_tpb.FP64)
-    solve("mixed", eps=1e-4, precision=sbd_tpb.MIXED)
-    pc, train = train_preconditioner(h.device)
+    par = lambda **kw: sbd_tpb.default_params(max_it=40, max_nb=8, **kw)  # noqa: E731
+    out["fp64_reference"] = _solve(h, par(eps=1e-6, precision=sbd_tpb.FP64), runs=1)
+    out["fp64"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.FP64))
+    out["mixed"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.MIXED))
     h.set_preconditioner(pc)
-    solve("mixed_learned", eps=1e-4, precision=sbd_tpb.MIXED, preconditioner=sbd_tpb.PRECOND_LEARNED)
+    out["mixed_learned"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.MIXED,
+                                         preconditioner=sbd_tpb.PRECOND_LEARNED))
     h.set_preconditioner(None)
-    pc.close()
     e_ref = out["fp64_reference"]["energy"]
     for k in ("fp64", "mixed", "mixed_learned"):
         out[k]["abs_energy_error_vs_fp64_reference"] = abs(out[k]["energy"] - e_ref)
-    out["learned_training"] = train
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["speedup_mixed_learned_vs_fp64"] = out["fp64"]["seconds"] / out["mixed_learned"]["seconds"]
     out["note"] = ("training (pairs from the 12- and 24-orbital problems) is timed separately and not "
-                   "part of the solve times; seconds = the faster of seconds_runs (two runs of each "
+                   "part of the solve times; seconds = the median of seconds_runs (three runs of each "
                    "compared solve)")
     return out
+
+
+def learned_cfg4(device, pc):
+    """The learned against the diagonal Davidson correction on the 28-orbital, 9+9-electron,
+    10,000 x 10,000-string problem (100M determinants): FP64 and mixed precision, to residual
+    1e-4 (|dE| below 1e-6 Ha), median of three solves each, step counts of every run."""
+    import sbd_tpb
+    import synth
+    h = sbd_tpb.Handle(device)
+    h.set_problem(synth.make_problem("sci28"))
+    h.set_preconditioner(pc)
+    out = {}
+    for prec, tag in ((sbd_tpb.FP64, "fp64"), (sbd_tpb.MIXED, "mixed")):
+        for pre, ptag in ((sbd_tpb.PRECOND_DIAGONAL, "diagonal"), (sbd_tpb.PRECOND_LEARNED, "learned")):
+            out[f"{tag}_{ptag}"] = _solve(h, sbd_tpb.default_params(max_it=40, max_nb=8, eps=1e-4,
+                                                                   precision=prec, preconditioner=pre))
+    ref = _solve(h, sbd_tpb.default_params(max_it=40, max_nb=8, eps=1e-6, precision=sbd_tpb.FP64), runs=1)
+    for v in out.values():
+        v["abs_energy_error_vs_fp64_reference"] = abs(v["energy"] - ref["energy"])
+    out["fp64_reference_energy"] = ref["energy"]
+    for tag in ("fp64", "mixed"):
+        d, l_ = out[f"{tag}_diagonal"], out[f"{tag}_learned"]
+        out[f"{tag}_learned_over_diagonal"] = {"steps": l_["sigma_steps"] / d["sigma_steps"],
+                                               "seconds": l_["seconds"] / d["seconds"]}
+    h.set_preconditioner(None)
+    h.close()
+    return out
+
+
+def timed_sigma(h, x, y, steps, warmup, stream, pg=None):
+    """Device ms of `steps` back-to-back sigma calls on vectors resident in HBM (after `warmup`
+    untimed ones), bracketed by barriers and synchronisation; kernel launches inside."""
+    import torch
+    for _ in range(warmup):
+        h.sigma_device(x, y)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = h.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        h.sigma_device(x, y)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), h.kernel_launches() - launches0
+
+
+def kernel_breakdown(h, prob, x, y, esz, reps):
+    """Per-stage device ms of sigma (CUDA events between the stages) and each stage's algorithmic
+    bytes: a same-spin pass reads X and read-modify-writes or writes its outputs, 3 N s in all
+    (alpha: read C, write sigma, write C^T; beta: read C^T, sigma read-modify-write), plus its
+    table program read once; the alpha pass also reads H_ii (N s_h); the sparse alpha-beta stage
+    read-modify-writes the sigma rows of alpha strings with singles and reads its singles' C rows."""
+    kern = []
+    for _ in range(reps):
+        h.sigma_device(x, y)
+        kern.append(h.last_sigma_kernels())
+    kern = np.array(kern).mean(axis=0)
+    N = prob.ndet
+
+    def table_bytes(singles, doubles):
+        ns, nd = int(h.table(singles)[1].size), int(h.table(doubles)[1].size)
+        return ns * (4 + esz + 4) + nd * (4 + esz) + 8 * (len(prob.astr) + 1)
+    names = ["sigma_block_kernel<alpha>", "sigma_block_kernel<beta>", "alpha_beta_term"][:len(kern)]
+    per = [3 * N * esz + N * esz + table_bytes(0, 1), 3 * N * esz + table_bytes(2, 3),
+           2 * N * esz + table_bytes(0, 2) // 4][:len(kern)]
+    return names, kern, per
 
 
 def run_ours(args, world, rank, local, pg):
@@ -419,65 +529,38 @@ def run_ours(args, world, rank, local, pg):
     t1 = time.time()
     h.build_tables()
     t_tables = time.time() - t1
-    dt = torch.float32 if args.precision == "mixed" else torch.float64
-    esz = 4 if dt == torch.float32 else 8
-    gen = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
-    x = torch.randn(N, dtype=dt, device=f"cuda:{local}", generator=gen)
-    x /= torch.linalg.vector_norm(x)
-    y = torch.empty_like(x)
     stream = torch.cuda.ExternalStream(h.stream(), device=f"cuda:{local}")
+    gen = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
+    head_dt = torch.float64 if args.precision == "fp64" else torch.float32
+    other_dt = torch.float32 if head_dt == torch.float64 else torch.float64
 
-    def barrier():
-        if pg is not None:
-            pg.barrier()
+    def vectors(dt):
+        x = torch.randn(N, dtype=dt, device=f"cuda:{local}", generator=gen)
+        x /= torch.linalg.vector_norm(x)
+        return x, torch.empty_like(x)
 
-    for _ in range(args.warmup):
-        h.sigma_device(x, y)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    launches0 = h.kernel_launches()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    # headline sigma
+    x, y = vectors(head_dt)
+    esz = x.element_size()
     with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            h.sigma_device(x, y)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms_total = ev0.elapsed_time(ev1)
-    launches = h.kernel_launches() - launches0
-    barrier()
+        ms_total, launches = timed_sigma(h, x, y, args.steps, args.warmup, stream, pg)
+    if pg is not None:
+        pg.barrier()
     ms_max, value = replica_throughput(pg, ms_total, N * args.steps, world, device=f"cuda:{local}")
     ms_step = ms_max / args.steps
 
-    # per-kernel times of the same sigma (separate pass: reading them synchronises each call)
-    kern = []
-    for _ in range(max(3, min(args.steps, 10))):
-        h.sigma_device(x, y)
-        kern.append(h.last_sigma_kernels())
-    kern = np.array(kern).mean(axis=0)
-    # algorithmic bytes of each pass: 3 N s (alpha: read C, write sigma, write C^T; beta: read
-    # C^T, sigma read-modify-write) plus its sigma-program tables read once
-    def table_bytes(singles, doubles):
-        ns, nd = int(h.table(singles)[1].size), int(h.table(doubles)[1].size)
-        return ns * (4 + esz + 4) + nd * (4 + esz) + 8 * (len(prob.astr) + 1)
-    bytes_alpha = 3 * N * esz + table_bytes(0, 1)
-    bytes_beta = 3 * N * esz + table_bytes(2, 3)
-    # third timed kernel: the alpha-beta term (sparse kernel, or the dense gather/contract/scatter)
-    names = ["sigma_block_kernel<alpha>", "sigma_block_kernel<beta>", "alpha_beta_term"][:len(kern)]
-    # sparse alpha-beta: sigma rows of alpha strings with singles read-modified-written, their
-    # singles' C rows read once
-    bytes_ab = 2 * N * esz + table_bytes(0, 2) // 4
-    per = [bytes_alpha, bytes_beta, bytes_ab][:len(kern)]
+    names, kern, per = kernel_breakdown(h, prob, x, y, esz, max(3, min(args.steps, 10)))
     dom = int(np.argmax(kern))
     pk = peaks()
     achieved = per[dom] / (kern[dom] * 1e-3) / 1e9
-    # DRAM bytes per determinant of each pass from the ncu capture at 10^8 determinants (FP32,
-    # profiles/sigma_kernels_sci28_fp32.md), scaled to this workload's determinants
-    traffic_per_det = {"sigma_block_kernel<alpha>": 17.69, "sigma_block_kernel<beta>": 12.60}
-    traffic = (traffic_per_det[names[dom]] * N / 1e9
-               if dt == torch.float32 and names[dom] in traffic_per_det else None)
+    # DRAM bytes per determinant of the dominant pass, from one ncu capture of that kernel at
+    # 10^8 determinants (norb=28), scaled by determinants: DRAM traffic of these passes grows in
+    # proportion to the vectors they stream
+    traffic_per_det = {(8, "sigma_block_kernel<alpha>"): TRAFFIC_F64_ALPHA,
+                       (8, "sigma_block_kernel<beta>"): TRAFFIC_F64_BETA,
+                       (4, "sigma_block_kernel<alpha>"): 17.69, (4, "sigma_block_kernel<beta>"): 12.60}
+    tpd = traffic_per_det.get((esz, names[dom]))
+    traffic = tpd * N / 1e9 if tpd else None
     roofline = {"kernel": names[dom], "bound": "hbm", "achieved": achieved,
                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                 "traffic": traffic, "traffic_unit": "GB per launch",
@@ -489,13 +572,32 @@ def run_ours(args, world, rank, local, pg):
     # end to end through the reference-facing C ABI: host buffers, copies and sign passes timed
     e2e = None
     if not args.no_e2e:
-        e2e = end_to_end(h, x, N, dt, esz, world)
+        e2e = end_to_end(h, x, N, head_dt, esz, world)
 
-    solve = None
+    # the other precision's sigma, same timing
+    del x, y
+    torch.cuda.empty_cache()
+    xo, yo = vectors(other_dt)
+    ms_o, _ = timed_sigma(h, xo, yo, args.steps, args.warmup, stream, pg)
+    names_o, kern_o, per_o = kernel_breakdown(h, prob, xo, yo, xo.element_size(), max(3, min(args.steps, 10)))
+    other = {"dtype": "f32 vectors, f64 accumulate" if other_dt == torch.float32 else "f64",
+             "value": world * N * args.steps / (ms_o * 1e-3) / 1e9, "unit": "GDets/s",
+             "ms_per_step": ms_o / args.steps,
+             "kernel_ms": {names_o[i]: float(kern_o[i]) for i in range(len(kern_o))},
+             "hbm_frac": {names_o[i]: per_o[i] / (kern_o[i] * 1e-3) / 1e9 / pk["hbm_gbs"]
+                          for i in range(len(kern_o))}}
+    del xo, yo
+    torch.cuda.empty_cache()
+
+    solve = cfg4 = train = None
     if not args.no_solve and world == 1:
-        del x, y
-        torch.cuda.empty_cache()
-        solve = time_to_solution(h, args)
+        pc, train = train_preconditioner(h.device)
+        solve = time_to_solution(h, args, pc)
+        solve["learned_training"] = train
+        if not args.no_cfg4:
+            h.free_vectors()
+            cfg4 = learned_cfg4(h.device, pc)
+        pc.close()
 
     strings = None
     if not args.no_carryover and world == 1:
@@ -508,19 +610,20 @@ def run_ours(args, world, rank, local, pg):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_reference_sigma(args.workload, args.cpu_sample_seconds)
+        h.free_vectors()
+        r = cpu_reference_sigma_full(args.workload)
         if r is not None:
-            t = sum(r["sigma_s"]) / len(r["sigma_s"])
-            cpu = {"value": r["ndet"] / t / 1e9, "unit": "GDets/s", "cores": r["threads"],
-                   "kind": "reference",
-                   "sample": f"first {r['amax']} of {r['nstrings']} alpha x all beta strings "
-                             f"({r['ndet']} dets), one reference sbd::mult (tpb/mult.h:625-881)"}
+            cpu = {"value": r["ndet"] / r["sigma_s"] / 1e9, "unit": "GDets/s", "cores": r["threads"],
+                   "kind": "reference", "seconds": r["sigma_s"],
+                   "sample": f"the whole problem ({cnt} x {cnt} strings, {r['ndet']} determinants, "
+                             f"every connection), one call of the reference's sbd::mult "
+                             f"(tpb/mult.h:625-881), FP64"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GDets/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 vectors, f64 accumulate" if dt == torch.float32 else "f64",
+            "dtype": "f64" if head_dt == torch.float64 else "f32 vectors, f64 accumulate",
             "data": "synthetic (seeded integrals 1729, strings 137)",
             "config": {"workload": f"{args.workload}: norb={L}, {n}+{n} electrons, {cnt} x {cnt} strings",
                        "determinants": N, "precision": args.precision,
@@ -528,7 +631,8 @@ def run_ours(args, world, rank, local, pg):
                        "l2": "inputs larger than L2 (vector of %.2f GB)" % (N * esz / 1e9),
                        "tables_s": t_tables, "setup_s": t1 - t0},
             "gpu_launches": launches, "clocks": clocks.summary(), "roofline": roofline, "e2e": e2e,
-            "cpu_baseline": cpu, "time_to_solution": solve, "carryover": carry, "strings": strings,
+            "cpu_baseline": cpu, "sigma_f32" if other_dt == torch.float32 else "sigma_f64": other,
+            "time_to_solution": solve, "learned_cfg4": cfg4, "carryover": carry, "strings": strings,
         }
         print(json.dumps(line), flush=True)
     h.close()

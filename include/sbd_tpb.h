@@ -217,7 +217,8 @@ SBD_TPB_API int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigm
  * HBM (their own eigensolver, benchmarks).  dtype 0 = double, 1 = float; convention 0 = the
  * reference's (interleaved determinant, as sbd_tpb_sigma), 1 = the library's internal separated
  * convention (alpha creators before beta creators: x_sep = D x_ref with
- * D = (-1)^#{(p in Ia, q in Ib) : q < p}), which skips the two sign passes.  Same accumulate rule. */
+ * D = (-1)^#{(p in Ia, q in Ib) : q < p}), which skips the two sign passes.  Same accumulate rule;
+ * in convention 1, C and sigma must be distinct buffers (SBD_TPB_ERR_INVALID otherwise). */
 SBD_TPB_API int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
                                      int accumulate, int convention);
 
@@ -227,13 +228,15 @@ SBD_TPB_API int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sig
 /* sigma (+)= H*C on device vectors in the separated convention (as sbd_tpb_sigma_device with
  * convention 1) that allocates no device memory.  No counterpart in the reference: it serves
  * callers that cannot have a library call cudaMalloc under them -- a code that has already
- * reserved the card's memory through its own pool, or work issued inside stream capture.  The
- * C^T staging lives in a static device array of SBD_TPB_NOALLOC_SCRATCH_BYTES that every GPU
- * loading the library holds until exit; ndet * element size beyond it is rejected with
- * SBD_TPB_ERR_INVALID.  All calls on a device share that array (nothing in it must start at
- * zero), so calls whose kernels overlap on the GPU race: serialise them.  The first call on a
- * device looks up the array's address (cudaGetSymbolAddress) and reads the table offsets back
- * once: make it before any stream capture.  The alpha-beta terms always use the direct loop. */
+ * reserved the card's memory through its own pool, or one whose memory policy forbids
+ * allocations after set-up.  The C^T staging lives in a static device array of
+ * SBD_TPB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit;
+ * ndet * element size beyond it is rejected with SBD_TPB_ERR_INVALID, as are C == sigma and
+ * tables that sbd_tpb_build_tables did not finish.  All calls on a device share that array
+ * (nothing in it must start at zero), so calls whose kernels overlap on the GPU race: serialise
+ * them.  The first call on a device looks up the array's address (cudaGetSymbolAddress) and
+ * keeps it for the process: make that first call before any stream capture, and do not call it
+ * on a device after cudaDeviceReset.  The alpha-beta terms always use the direct loop. */
 SBD_TPB_API int sbd_tpb_sigma_noalloc(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
                                       int accumulate);
 
@@ -283,6 +286,12 @@ SBD_TPB_API int sbd_tpb_last_sigma_kernels(sbd_tpb_handle *h, double *ms, int ma
 
 /* Number of kernel launches the library has issued on this handle (for accounting). */
 SBD_TPB_API uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h);
+
+/* Release the handle's cached work memory: the Davidson N-vectors kept between solves, the
+ * sigma C^T staging and the sign-conversion vectors.  Tables, diagonal and the problem stay;
+ * the next call that needs the work memory allocates it again.  No counterpart in the
+ * reference, whose solver frees its vectors at the end of each call. */
+SBD_TPB_API int sbd_tpb_release_work(sbd_tpb_handle *h);
 
 /* ---- learned Davidson preconditioner ------------------------------------------------------
  * No counterpart in the reference, whose only correction is the diagonal one

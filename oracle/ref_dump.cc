@@ -11,6 +11,9 @@
 //                         off = CSR offsets (u64), ket = ket string index (u64), cran = labels (i32)
 //   hii.f64               makeQChamDiagTerms (tpb/qcham.h:290-340)
 //   sigma_in.f64 / sigma_out.f64   one application of mult (tpb/mult.h:625-881) to a seeded vector
+//                         (--sigma_seed: normal deviates; --sigma_hash: the closed-form vector
+//                         x_i = ((i * 0x9E3779B97F4A7C15 mod 2^64) >> 11) / 2^53 - 1/2, which a
+//                         test regenerates exactly at any size without storing it)
 //   davidson.txt / W.f64  Davidson (tpb/davidson.h:667-930) from the HF start, energy as in
 //                         tpb/sbdiag.h:431-469
 //   rdm1.f64 / rdm2.f64   Correlation (tpb/correlation.h:378-664)
@@ -28,7 +31,7 @@
 //                         trailing strings (a null dereference in MpiBcast)
 //
 // Usage: ref_dump --fcidump F --adetfile A [--bdetfile B] [--bit_length 20] --out DIR
-//                 [--sigma_seed S] [--davidson IT NB TOL] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
+//                 [--sigma_seed S | --sigma_hash] [--davidson IT NB TOL] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
 //                 [--lanczos IT NB TOL]
 // The reference headers rely on their includer for these (as its app main.cc does).
 #include <chrono>
@@ -92,6 +95,7 @@ int main(int argc, char **argv) {
   std::string fcidumpfile, adetfile, bdetfile, out = ".";
   size_t bit_length = 20;
   long sigma_seed = -1;
+  bool sigma_hash = false;
   int dav_it = 0, dav_nb = 0;
   double dav_tol = 1e-8;
   bool do_rdm = false;
@@ -106,6 +110,7 @@ int main(int argc, char **argv) {
     else if (a == "--bit_length") bit_length = std::atoi(argv[++i]);
     else if (a == "--out") out = argv[++i];
     else if (a == "--sigma_seed") sigma_seed = std::atol(argv[++i]);
+    else if (a == "--sigma_hash") sigma_hash = true;
     else if (a == "--davidson") {
       dav_it = std::atoi(argv[++i]);
       dav_nb = std::atoi(argv[++i]);
@@ -186,11 +191,16 @@ int main(int argc, char **argv) {
                           t_comm);
   write_raw(out + "/hii.f64", hii.data(), hii.size());
 
-  if (sigma_seed >= 0) {
-    std::mt19937_64 g(static_cast<uint64_t>(sigma_seed));
-    std::normal_distribution<double> nd(0.0, 1.0);
+  if (sigma_seed >= 0 || sigma_hash) {
     std::vector<double> win(hii.size()), wout(hii.size(), 0.0);
-    for (auto &x : win) x = nd(g);
+    if (sigma_hash) {
+      for (size_t i = 0; i < win.size(); ++i)
+        win[i] = (double)((uint64_t(i) * 0x9E3779B97F4A7C15ull) >> 11) * 0x1p-53 - 0.5;
+    } else {
+      std::mt19937_64 g(static_cast<uint64_t>(sigma_seed));
+      std::normal_distribution<double> nd(0.0, 1.0);
+      for (auto &x : win) x = nd(g);
+    }
     sbd::mult(hii, win, wout, adet, bdet, bit_length, static_cast<size_t>(L), 1, 1, helper, I0,
               I1, I2, h_comm, b_comm, t_comm);
     write_raw(out + "/sigma_in.f64", win.data(), win.size());

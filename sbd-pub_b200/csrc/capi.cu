@@ -213,6 +213,7 @@ int sbd_tpb_build_tables(sbd_tpb_handle *h) {
   TPB_HANDLE(h);
   if (!h->have_strings) return fail(SBD_TPB_ERR_STATE, "set strings before building tables");
   TPB_CHECK(build_excitation_tables(h));
+  TPB_CHECK(prepare_block_sizes(h));
   TPB_CHECK(build_sigma_programs(h));
   TPB_CHECK(compute_diagonal(h));
   TPB_CHECK(ab_dense_setup(h, ab_dense_worthwhile(h) ? 1 : 0));
@@ -331,6 +332,8 @@ int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtyp
                       : sbd_tpb_sigma_f32(h, (const float *)C, (float *)sigma, accumulate, SBD_TPB_DEVICE);
   }
   if (convention != 1) return fail(SBD_TPB_ERR_INVALID, "convention must be 0 or 1");
+  // the passes read C while they write sigma
+  if (C == sigma) return fail(SBD_TPB_ERR_INVALID, "sigma_device: C and sigma must be distinct buffers");
   if (dtype == 0) TPB_CHECK(sigma_sep<double>(h, (const double *)C, (double *)sigma, accumulate));
   else TPB_CHECK(sigma_sep<float>(h, (const float *)C, (float *)sigma, accumulate));
   TPB_CUDA(cudaEventSynchronize(h->ev1));
@@ -503,5 +506,17 @@ int sbd_tpb_last_sigma_kernels(sbd_tpb_handle *h, double *ms, int max_n) {
 }
 
 uint64_t sbd_tpb_kernel_launches(sbd_tpb_handle *h) { return h ? h->launches : 0; }
+
+int sbd_tpb_release_work(sbd_tpb_handle *h) {
+  TPB_HANDLE(h);
+  TPB_CUDA(cudaSetDevice(h->device));
+  TPB_CUDA(cudaStreamSynchronize(h->stream));
+  pool_clear(h);
+  free_tmps(h);
+  if (h->d_ct) cudaFree(h->d_ct);
+  h->d_ct = nullptr;
+  h->ct_bytes = 0;
+  return SBD_TPB_OK;
+}
 
 }  // extern "C"

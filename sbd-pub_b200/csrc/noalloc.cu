@@ -1,14 +1,14 @@
 // sbd_tpb_sigma_noalloc: sigma on device vectors without any device allocation.
 //
 // Some callers cannot let a library call cudaMalloc while they run: a code that has reserved
-// nearly all of HBM up front through its own pool (a framework caching allocator, a solver
-// that sized its Krylov space to the card), where one more cudaMalloc fails or forces a
-// pool flush; and code running inside a region where allocation is not permitted or would
-// not be recorded, such as CUDA stream capture.  The regular sigma entry points allocate their
-// C^T staging buffer (and the dense alpha-beta work arrays) lazily on first use; this variant
-// uses instead a fixed scratch array that lives in the library's own device image and
-// evaluates the alpha-single x beta-single terms with the direct loop, which needs no work
-// arrays.
+// nearly all of HBM up front through its own pool (a framework caching allocator, a solver that
+// sized its Krylov space to the card), where one more cudaMalloc fails or forces the pool to
+// flush, and a host code whose memory policy forbids allocations after its set-up phase.  The
+// regular sigma entry points allocate their C^T staging buffer (and the dense alpha-beta work
+// arrays) lazily on first use; this variant uses instead a fixed scratch array that lives in the
+// library's own device image, and evaluates the alpha-single x beta-single terms with the direct
+// loop, which needs no work arrays.  Everything else it reads (tables, sigma programs, the
+// diagonal, the per-block table sizes) is built by sbd_tpb_build_tables.
 //
 // Limits and sharing rules:
 //   * the scratch holds C^T: ndet * sizeof(element) must not exceed
@@ -20,8 +20,9 @@
 //     reads it), but two calls whose kernels overlap on the GPU race on it: serialise them (one
 //     stream, or events between streams);
 //   * the first call on each device looks up the array's device address with
-//     cudaGetSymbolAddress (which may load the library's device code), so make that first call
-//     before any stream capture.
+//     cudaGetSymbolAddress (which may load the library's device code) and keeps it for the rest
+//     of the process, so make that first call before any stream capture; a cudaDeviceReset
+//     invalidates the kept address, so do not call this entry point on a device after resetting it.
 #include <mutex>
 #include <string>
 
@@ -62,7 +63,13 @@ extern "C" int sbd_tpb_sigma_noalloc(sbd_tpb_handle *h, const void *C, void *sig
   if (!h) return fail(SBD_TPB_ERR_INVALID, "null handle");
   if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
   if (!C || !sigma) return fail(SBD_TPB_ERR_INVALID, "null vector");
+  if (C == sigma)
+    return fail(SBD_TPB_ERR_INVALID, "sbd_tpb_sigma_noalloc: C and sigma must be distinct buffers");
   if (dtype != 0 && dtype != 1) return fail(SBD_TPB_ERR_INVALID, "dtype must be 0 (double) or 1 (float)");
+  // the per-block table sizes are read back at table build; without them the launch would need a
+  // synchronous copy here
+  if (h->blk_for != (const void *)h->ta_d.ket)
+    return fail(SBD_TPB_ERR_STATE, "sbd_tpb_sigma_noalloc: table block sizes missing; rebuild the tables");
   const size_t esz = dtype == 0 ? sizeof(double) : sizeof(float);
   const size_t need = h->ndet() * esz;
   if (need > kScratchBytes)

@@ -522,29 +522,40 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   }
 }
 
-// Most entries of any kBlkRows-row block of a CSR table (shared-memory staging size).
-uint32_t max_block_entries(const ExTable &t, size_t n) {
+// Most entries of any kBlkRows-row block of a CSR table of n rows (shared-memory staging size).
+int max_block_entries(const ExTable &t, size_t n, uint32_t *out) {
+  *out = 0;
+  if (n == 0) return SBD_TPB_OK;
   std::vector<uint32_t> off(n + 1);
-  if (n == 0 || cudaMemcpy(off.data(), t.off, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost) !=
-                    cudaSuccess)
-    return 0;
+  TPB_CUDA(cudaMemcpy(off.data(), t.off, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost));
   uint32_t mx = 0;
   for (size_t r = 0; r < n; r += kBlkRows) mx = std::max(mx, off[std::min(n, r + kBlkRows)] - off[r]);
-  return mx;
+  *out = mx;
+  return SBD_TPB_OK;
 }
 
-// Host-side facts about the tables that size the sigma launches: the most table entries of any
-// kBlkRows-row block (shared-memory staging) and, when want_ab_lists, the alpha rows and beta
+// The most table entries of any kBlkRows-row block of each table (the shared-memory staging of
+// the sigma kernels), read back once per table build; blk_for records the tables they describe
+// and is set only when all four were read.
+int prepare_block_sizes(sbd_tpb_handle *h) {
+  if (h->blk_for == (const void *)h->ta_d.ket) return SBD_TPB_OK;
+  const size_t na = h->astr.size(), nb = h->bstr.size();
+  uint32_t m[4];
+  TPB_CHECK(max_block_entries(h->ta_d, na, &m[0]));
+  TPB_CHECK(max_block_entries(h->ta_s, na, &m[1]));
+  TPB_CHECK(max_block_entries(h->tb_d, nb, &m[2]));
+  TPB_CHECK(max_block_entries(h->tb_s, nb, &m[3]));
+  for (int i = 0; i < 4; i++) h->blk_max[i] = m[i];
+  h->blk_for = h->ta_d.ket;
+  return SBD_TPB_OK;
+}
+
+// Host-side facts about the tables that size the sigma launches: the per-block table sizes
+// (prepare_block_sizes, done at table build) and, when want_ab_lists, the alpha rows and beta
 // columns that have singles (the sparse alpha-beta launch).  Computed once per table build.
 int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
   const size_t na = h->astr.size(), nb = h->bstr.size();
-  if (h->blk_for != (const void *)h->ta_d.ket) {
-    h->blk_max[0] = max_block_entries(h->ta_d, na);
-    h->blk_max[1] = max_block_entries(h->ta_s, na);
-    h->blk_max[2] = max_block_entries(h->tb_d, nb);
-    h->blk_max[3] = max_block_entries(h->tb_s, nb);
-    h->blk_for = h->ta_d.ket;
-  }
+  TPB_CHECK(prepare_block_sizes(h));
   if (want_ab_lists && !h->d_ab_rows && na > 0 && nb > 0) {
     std::vector<uint32_t> ao(na + 1), bo(nb + 1), rows;
     TPB_CUDA(cudaMemcpy(ao.data(), h->ta_s.off, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToHost));

@@ -39,7 +39,7 @@ EXPORTED = [
     "sbd_tpb_destroy", "sbd_tpb_set_hamiltonian", "sbd_tpb_set_strings", "sbd_tpb_build_tables",
     "sbd_tpb_table_size", "sbd_tpb_get_table", "sbd_tpb_diagonal", "sbd_tpb_sigma",
     "sbd_tpb_sigma_f32", "sbd_tpb_sigma_device", "sbd_tpb_sigma_noalloc", "sbd_tpb_davidson", "sbd_tpb_rdm", "sbd_tpb_stream",
-    "sbd_tpb_last_sigma_ms", "sbd_tpb_last_sigma_kernels", "sbd_tpb_kernel_launches",
+    "sbd_tpb_last_sigma_ms", "sbd_tpb_last_sigma_kernels", "sbd_tpb_kernel_launches", "sbd_tpb_release_work",
     "sbd_tpb_precond_create", "sbd_tpb_precond_destroy", "sbd_tpb_precond_collect",
     "sbd_tpb_precond_num_samples", "sbd_tpb_precond_train", "sbd_tpb_precond_evaluate",
     "sbd_tpb_precond_get_params", "sbd_tpb_precond_set_params", "sbd_tpb_precond_gradients",
@@ -141,6 +141,7 @@ def lib():
     L.sbd_tpb_last_sigma_kernels.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
     L.sbd_tpb_kernel_launches.restype = C.c_uint64
     L.sbd_tpb_kernel_launches.argtypes = [vp]
+    L.sbd_tpb_release_work.argtypes = [vp]
     L.sbd_tpb_precond_create.argtypes = [C.c_int, C.c_uint64, C.POINTER(vp)]
     L.sbd_tpb_precond_destroy.argtypes = [vp]
     L.sbd_tpb_precond_collect.argtypes = [vp, vp, C.POINTER(Params), C.c_size_t, C.c_int,
@@ -270,9 +271,25 @@ class Handle:
         _check(fn(self.h, _ptr(C_), _ptr(out), int(accumulate), DEVICE if dev else HOST))
         return out
 
+    def _device_pair(self, x, y) -> int:
+        """dtype code (0 float64, 1 float32) of two torch CUDA N-vectors the device entry points
+        may read and write: same dtype, one of the two, ndet elements, contiguous, on the
+        handle's device, distinct buffers."""
+        import torch
+        if x.dtype not in (torch.float64, torch.float32) or y.dtype != x.dtype:
+            raise TpbError(ERR_INVALID, f"sigma vectors must both be float64 or float32 (got {x.dtype}, {y.dtype})")
+        for t in (x, y):
+            if not t.is_cuda or t.device.index != self.device:
+                raise TpbError(ERR_INVALID, f"sigma vectors must live on cuda:{self.device}")
+            if not t.is_contiguous() or t.numel() != self.problem.ndet:
+                raise TpbError(ERR_INVALID, f"sigma vectors must be contiguous with {self.problem.ndet} elements")
+        if x.data_ptr() == y.data_ptr():
+            raise TpbError(ERR_INVALID, "sigma input and output must be distinct buffers")
+        return 1 if x.dtype == torch.float32 else 0
+
     def sigma_device(self, x, y, accumulate=False, separated=True):
         """sigma on torch CUDA tensors; separated=True keeps the library's internal convention."""
-        dt = 1 if str(x.dtype) == "torch.float32" else 0
+        dt = self._device_pair(x, y)
         _check(lib().sbd_tpb_sigma_device(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate),
                                           1 if separated else 0))
         return y
@@ -280,7 +297,7 @@ class Handle:
     def sigma_noalloc(self, x, y, accumulate=False):
         """sigma into caller-owned torch CUDA tensors without any device allocation by the
         library (separated convention, fixed 16 MiB scratch; see sbd_tpb_sigma_noalloc)."""
-        dt = 1 if str(x.dtype) == "torch.float32" else 0
+        dt = self._device_pair(x, y)
         _check(lib().sbd_tpb_sigma_noalloc(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate)))
         return y
 
@@ -296,6 +313,10 @@ class Handle:
 
     def kernel_launches(self) -> int:
         return int(lib().sbd_tpb_kernel_launches(self.h))
+
+    def free_vectors(self):
+        """Release the cached work memory (Davidson vectors, sigma staging): sbd_tpb_release_work."""
+        _check(lib().sbd_tpb_release_work(self.h))
 
     def stream(self) -> int:
         return lib().sbd_tpb_stream(self.h) or 0

@@ -57,6 +57,12 @@ CASES = {
     "syn12_co": dict(synthetic=(12, 5, 5, 200, 150, 31), davidson=(10, 10, 1e-10), rdm=False, full=True,
                      carryover=(0.25, 1e-4, 1e-5), lanczos=(3, 30, 1e-10)),
     "fci12": dict(synthetic_named="fci12", davidson=(10, 10, 1e-8), rdm=False, full=False),
+    # the benchmark's larger selected-CI workloads (synthetic_named = a synth.CONFIGS entry): sigma
+    # of the closed-form vector (ref_dump --sigma_hash), so a test regenerates its input at any size;
+    # the 16M-determinant set also carries the reference's FP64 Davidson energy.  Only samples and
+    # checksums of the N-vectors are stored.
+    "sci24": dict(synthetic_named="sci24", davidson=(40, 10, 1e-6), rdm=False, full=False, sigma_hash=True),
+    "sci32": dict(synthetic_named="sci32", davidson=None, rdm=False, full=False, sigma_hash=True),
 }
 
 
@@ -75,11 +81,13 @@ def run_case(name: str, spec: dict, out_dir: str):
             synth.write_strings(fa, synth.sample_strings(L, n, cnt), L)
         else:
             fd, fa = spec["fcidump"], spec["adet"]
-        cmd = [DUMP, "--fcidump", fd, "--adetfile", fa, "--out", tmp, "--sigma_seed", "7"]
+        cmd = [DUMP, "--fcidump", fd, "--adetfile", fa, "--out", tmp]
+        cmd += ["--sigma_hash"] if spec.get("sigma_hash") else ["--sigma_seed", "7"]
         if bdet:
             cmd += ["--bdetfile", bdet]
-        it, nb, tol = spec["davidson"]
-        cmd += ["--davidson", str(it), str(nb), repr(tol)]
+        if spec["davidson"]:
+            it, nb, tol = spec["davidson"]
+            cmd += ["--davidson", str(it), str(nb), repr(tol)]
         if spec["rdm"]:
             cmd += ["--rdm"]
         if "carryover" in spec:
@@ -108,12 +116,15 @@ def run_case(name: str, spec: dict, out_dir: str):
                 data[f"t{t}_{k}_ket"] = ket
                 data[f"t{t}_{k}_cran"] = cran
         for vec in ("hii", "sigma_in", "sigma_out", "W"):
+            if vec == "W" and not spec["davidson"]:
+                continue
             v = rd(f"{vec}.f64")
             if spec["full"]:
                 data[vec] = v
             data[vec + "_sample"] = v[idx]
             data[vec + "_sum"] = np.array([v.sum(), (v * v).sum(), np.abs(v).sum()])
-        data["energy"] = np.array([float(open(os.path.join(tmp, "davidson.txt")).read())])
+        if spec["davidson"]:
+            data["energy"] = np.array([float(open(os.path.join(tmp, "davidson.txt")).read())])
         if spec["rdm"]:
             r1, r2 = rd("rdm1.f64"), rd("rdm2.f64")
             data["rdm1"] = r1
@@ -142,8 +153,12 @@ def run_case(name: str, spec: dict, out_dir: str):
         _, _, h1, eri, core = synth.read_fcidump(fd)
         data["h1"], data["eri"], data["core"] = h1, eri, np.array([core])
         np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **data)
-        meta = dict(norb=L, na=len(astr), nb=len(bstr), energy=float(data["energy"][0]),
-                    davidson=list(spec["davidson"]), rdm=spec["rdm"], full=spec["full"])
+        meta = dict(norb=L, na=len(astr), nb=len(bstr), rdm=spec["rdm"], full=spec["full"],
+                    davidson=list(spec["davidson"]) if spec["davidson"] else None)
+        if spec["davidson"]:
+            meta["energy"] = float(data["energy"][0])
+        if spec.get("sigma_hash"):
+            meta["sigma_input"] = "hash"
         for k in ("published", "published_src"):
             if k in spec:
                 meta[k] = spec[k]

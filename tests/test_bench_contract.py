@@ -1,7 +1,8 @@
 """bench.py's reference arm (`--impl reference`): the reference's own CPU sigma (oracle/_ref/ref_bench,
-sbd::mult of tpb/mult.h:625-881) timed on bounded samples, printed as one JSON line with the keys of the
-benchmark contract.  Runs on the CPU, here on the 24-orbital workload with a 2-second sample; under
-torchrun with two ranks (gloo), rank 0 alone prints the line and the other rank exits 0 without work."""
+sbd::mult of tpb/mult.h:625-881) timed per step on a bra-row block of the whole problem (every
+connection of the block's rows), printed as one JSON line with the keys of the benchmark contract.
+Runs on the CPU, here on the 24-orbital workload with 1-second blocks; under torchrun with two ranks
+(gloo), rank 0 alone prints the line and the other rank exits 0 without work."""
 import json
 import os
 import socket
@@ -13,7 +14,7 @@ import pytest
 from conftest import ROOT
 
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
-ARGS = ["--impl", "reference", "--workload", "sci24", "--steps", "1", "--warmup", "0", "--cpu-sample-seconds", "2"]
+ARGS = ["--impl", "reference", "--workload", "sci24", "--steps", "1", "--warmup", "0", "--cpu-step-seconds", "1"]
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_BENCH), reason="oracle/_ref not built")
 
 
@@ -30,6 +31,10 @@ def _check_line(d, n_gpus):
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "GDets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the sample covers the whole problem's connections: blocks of whole alpha rows x all beta strings
+    assert d["config"]["determinants"] == 4000 * 4000
+    b = d["blocks"]
+    assert 1 <= b["rows"] <= 4000 and len(b["block_s"]) == d["steps"] + d["warmup"] and b["fixed_s"] >= 0
 
 
 @needs_ref
