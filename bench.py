@@ -44,9 +44,11 @@ sys.path.insert(0, os.path.join(ROOT, "sbd-pub_b200", "python"))
 
 METRIC = "sigma GDets/s; time to 1e-6 Ha: mixed+learned vs plain FP64, 1 B200"
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
-# DRAM bytes per determinant of the FP64 passes (ncu, 10^8 determinants, norb=28)
-TRAFFIC_F64_ALPHA = None
-TRAFFIC_F64_BETA = None
+# DRAM bytes (read + write) per determinant of one launch of the FP64 sigma passes, from an ncu
+# capture of both kernels at 10^8 determinants (norb=28, 10,000 x 10,000 strings): alpha
+# 1.781 + 1.566 GB, beta 1.719 + 0.765 GB
+TRAFFIC_F64_ALPHA = 33.47
+TRAFFIC_F64_BETA = 24.84
 
 
 def parse():

@@ -218,7 +218,12 @@ SBD_TPB_API int sbd_tpb_sigma_f32(sbd_tpb_handle *h, const float *C, float *sigm
  * reference's (interleaved determinant, as sbd_tpb_sigma), 1 = the library's internal separated
  * convention (alpha creators before beta creators: x_sep = D x_ref with
  * D = (-1)^#{(p in Ia, q in Ib) : q < p}), which skips the two sign passes.  Same accumulate rule;
- * in convention 1, C and sigma must be distinct buffers (SBD_TPB_ERR_INVALID otherwise). */
+ * in convention 1, C and sigma must be distinct buffers (SBD_TPB_ERR_INVALID otherwise).
+ * Convention 2 = convention 1 for an exchange-symmetric C (C[Ia, Ib] = C[Ib, Ia] over identical
+ * alpha and beta string lists, the sector of an HF-started singlet solve): the beta part of sigma
+ * is then the transpose of the alpha part, so it runs one gathering pass and a transpose-add
+ * (accumulate must be 0; SBD_TPB_ERR_STATE when the string lists differ).  The answer equals
+ * convention 1 up to rounding only for a symmetric C. */
 SBD_TPB_API int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtype,
                                      int accumulate, int convention);
 

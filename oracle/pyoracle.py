@@ -70,6 +70,10 @@ def lib():
         L.orc_free_tables.argtypes = [C.POINTER(Tables)]
         L.orc_sigma.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.POINTER(Tables), C.POINTER(Ham),
                                 _f64p, _f64p, _f64p]
+        L.orc_hash_vector.restype = C.c_double
+        L.orc_hash_vector.argtypes = [C.c_size_t]
+        L.orc_sigma_rows.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.POINTER(Tables), C.POINTER(Ham),
+                                     C.c_void_p, C.c_void_p, C.c_size_t, _f64p]
         L.orc_davidson.restype = C.c_int
         L.orc_davidson.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.POINTER(Tables), C.POINTER(Ham),
                                    _f64p, _f64p, C.c_int, C.c_int, C.c_double, C.c_int,
@@ -173,6 +177,12 @@ def excitations(bra: np.ndarray, ket: np.ndarray, L: int, ndiff: int, spin: int)
     return off, k[:n], c[: n * (2 if ndiff == 2 else 4)]
 
 
+def hash_vector(idx) -> np.ndarray:
+    """The closed-form test vector at the given indices (same bits as orc_hash_vector)."""
+    i = np.asarray(idx, dtype=np.uint64)
+    return ((i * np.uint64(0x9E3779B97F4A7C15)) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53 - 0.5
+
+
 class System:
     """Strings + Hamiltonian + tables: the oracle's view of one TPB problem."""
 
@@ -212,6 +222,19 @@ class System:
         out = np.zeros(self.na * self.nb)
         lib().orc_sigma(self.astr, self.na, self.bstr, self.nb, C.byref(self.t), C.byref(self.ham.h),
                         np.ascontiguousarray(hii, np.float64), np.ascontiguousarray(C_, np.float64), out)
+        return out
+
+    def sigma_rows(self, rows, C_: np.ndarray | None = None) -> np.ndarray:
+        """sigma at the determinant indices `rows` (orc_sigma_rows); C_ = None takes the closed-form
+        vector hash_vector(index), so no N-vector is needed."""
+        rows = np.ascontiguousarray(rows, np.uint64)
+        out = np.zeros(len(rows))
+        cptr = None
+        if C_ is not None:
+            C_ = np.ascontiguousarray(C_, np.float64)
+            cptr = C_.ctypes.data
+        lib().orc_sigma_rows(self.astr, self.na, self.bstr, self.nb, C.byref(self.t), C.byref(self.ham.h),
+                             cptr, rows.ctypes.data, len(rows), out)
         return out
 
     def davidson(self, max_it=10, max_nb=10, eps=1e-8, verbose=False, W0=None):

@@ -532,6 +532,48 @@ void orc_sigma(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
   }
 }
 
+/* The closed-form test vector x_i = ((i * 0x9E3779B97F4A7C15 mod 2^64) >> 11) / 2^53 - 1/2 (the
+ * input of the reference dumps made with --sigma_hash). */
+double orc_hash_vector(size_t i) {
+  return (double)(((uint64_t)i * 0x9E3779B97F4A7C15ull) >> 11) * 0x1p-53 - 0.5;
+}
+
+void orc_sigma_rows(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                    const orc_tables *t, const orc_ham *h, const double *C, const size_t *rows,
+                    size_t nrows, double *out) {
+  /* orc_sigma for the determinants rows[0..nrows) only, each added in the same order; H_ii from
+   * orc_zero_excite, C[k] from the array or, when C is NULL, orc_hash_vector(k) */
+#define CV(k) (C ? C[(k)] : orc_hash_vector((k)))
+#pragma omp parallel for schedule(dynamic, 1)
+  for (size_t r = 0; r < nrows; r++) {
+    const size_t bra = rows[r], ia = bra / nb, ib = bra % nb;
+    det128 d = interleave(astr[ia], bstr[ib]);
+    double acc = 0.0;
+    acc += orc_zero_excite(astr[ia], bstr[ib], h) * CV(bra);
+    for (uint64_t j = t->sa_off[ia]; j < t->sa_off[ia + 1]; j++)
+      acc += one_excite_det(&d, t->sa_cran[2 * j], t->sa_cran[2 * j + 1], h) * CV(t->sa_ket[j] * nb + ib);
+    for (uint64_t j = t->da_off[ia]; j < t->da_off[ia + 1]; j++) {
+      const int32_t *c = t->da_cran + 4 * j;
+      acc += two_excite_det(&d, c[0], c[1], c[2], c[3], h) * CV(t->da_ket[j] * nb + ib);
+    }
+    for (uint64_t j = t->sb_off[ib]; j < t->sb_off[ib + 1]; j++)
+      acc += one_excite_det(&d, t->sb_cran[2 * j], t->sb_cran[2 * j + 1], h) * CV(ia * nb + t->sb_ket[j]);
+    for (uint64_t j = t->db_off[ib]; j < t->db_off[ib + 1]; j++) {
+      const int32_t *c = t->db_cran + 4 * j;
+      acc += two_excite_det(&d, c[0], c[1], c[2], c[3], h) * CV(ia * nb + t->db_ket[j]);
+    }
+    for (uint64_t j = t->sa_off[ia]; j < t->sa_off[ia + 1]; j++) {
+      const size_t ja = t->sa_ket[j];
+      for (uint64_t k = t->sb_off[ib]; k < t->sb_off[ib + 1]; k++)
+        acc += two_excite_det(&d, t->sa_cran[2 * j], t->sb_cran[2 * k], t->sa_cran[2 * j + 1],
+                              t->sb_cran[2 * k + 1], h) *
+               CV(ja * nb + t->sb_ket[k]);
+    }
+    out[r] = acc;
+  }
+#undef CV
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* Davidson (tpb/davidson.h:667-930, framework/dm_vector.h:23-87)                              */
 /* ------------------------------------------------------------------------------------------ */

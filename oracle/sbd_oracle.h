@@ -98,6 +98,14 @@ void orc_sigma(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
                const orc_tables *t, const orc_ham *h, const double *hii, const double *C,
                double *sigma);
 
+/* The closed-form test vector ((i * 0x9E3779B97F4A7C15 mod 2^64) >> 11) / 2^53 - 1/2. */
+double orc_hash_vector(size_t i);
+/* sigma = H*C at the determinants rows[0..nrows) (index Ia*nb + Ib), reference sign convention,
+ * the terms added in orc_sigma's order; C = NULL takes the closed-form vector. */
+void orc_sigma_rows(const uint64_t *astr, size_t na, const uint64_t *bstr, size_t nb,
+                    const orc_tables *t, const orc_ham *h, const double *C, const size_t *rows,
+                    size_t nrows, double *out);
+
 /* Block Davidson for the lowest root (tpb/davidson.h:667-930) from W (in/out); the subspace
  * eigenproblem uses a cyclic Jacobi solver with eigenvalues sorted ascending.  Returns the
  * number of sigma applications; *energy is <W|H|W> after the loop as in tpb/sbdiag.h:431-469,

@@ -331,11 +331,18 @@ int sbd_tpb_sigma_device(sbd_tpb_handle *h, const void *C, void *sigma, int dtyp
     return dtype == 0 ? sbd_tpb_sigma(h, (const double *)C, (double *)sigma, accumulate, SBD_TPB_DEVICE)
                       : sbd_tpb_sigma_f32(h, (const float *)C, (float *)sigma, accumulate, SBD_TPB_DEVICE);
   }
-  if (convention != 1) return fail(SBD_TPB_ERR_INVALID, "convention must be 0 or 1");
+  if (convention != 1 && convention != 2) return fail(SBD_TPB_ERR_INVALID, "convention must be 0, 1 or 2");
   // the passes read C while they write sigma
   if (C == sigma) return fail(SBD_TPB_ERR_INVALID, "sigma_device: C and sigma must be distinct buffers");
-  if (dtype == 0) TPB_CHECK(sigma_sep<double>(h, (const double *)C, (double *)sigma, accumulate));
-  else TPB_CHECK(sigma_sep<float>(h, (const float *)C, (float *)sigma, accumulate));
+  if (convention == 2) {
+    if (accumulate) return fail(SBD_TPB_ERR_INVALID, "sigma_device: convention 2 does not accumulate");
+    if (dtype == 0) TPB_CHECK(sigma_sep_sym<double>(h, (const double *)C, (double *)sigma, 0.0));
+    else TPB_CHECK(sigma_sep_sym<float>(h, (const float *)C, (float *)sigma, 0.0));
+  } else if (dtype == 0) {
+    TPB_CHECK(sigma_sep<double>(h, (const double *)C, (double *)sigma, accumulate));
+  } else {
+    TPB_CHECK(sigma_sep<float>(h, (const float *)C, (float *)sigma, accumulate));
+  }
   TPB_CUDA(cudaEventSynchronize(h->ev1));
   TPB_CUDA(cudaEventElapsedTime(&h->last_sigma_ms, h->ev0, h->ev1));
   return SBD_TPB_OK;

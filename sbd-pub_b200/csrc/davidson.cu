@@ -175,7 +175,10 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
     cycle_steps = 0;
     for (int ib = 0; ib < nb; ib++) {
       const auto s0 = std::chrono::steady_clock::now();
-      TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
+      // S_ib is exactly exchange-symmetric under the projection (every correction is projected,
+      // every other operation is elementwise), so its sigma takes the one-pass symmetric form
+      if (sym) TPB_CHECK(sigma_sep_sym<T>(h, S[ib].p, HS[ib].p, shift));
+      else TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
       nsigma++;
       std::vector<const T *> cp(ib + 1);
       for (int k = 0; k <= ib; k++) cp[k] = S[k].p;

@@ -19,6 +19,7 @@
 #include <string>
 
 #include "tpb_common.cuh"
+#include "vecops.cuh"
 
 namespace sbdtpb {
 namespace {
@@ -138,7 +139,10 @@ struct BlockArgs {
 //     string's orbitals.
 //   beta pass: X = C^T.  Each thread adds its rows x VW results into sigma[Ia, Ib0 ...)
 //     (contiguous along Ib) for its columns Ia.
-template <typename T, bool kAlpha, bool kVec, int G, int M, bool OS>
+//   symmetric alpha pass (kSym, with kAlpha): for C = C^T over identical alpha and beta strings the
+//     beta part of sigma is the transpose of the alpha part, so the pass writes
+//     B = (H_ii - shift) C / 2 + (alpha part) and no C^T; sym_add then forms sigma = B + B^T.
+template <typename T, bool kAlpha, bool kVec, int G, int M, bool OS, bool kSym = false>
 __global__ void __launch_bounds__(kBlkThreads, M)
     sigma_block_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
   constexpr int VW = 16 / sizeof(T);
@@ -192,13 +196,13 @@ __global__ void __launch_bounds__(kBlkThreads, M)
   const bool full = ok[VW - 1];
 
   T acc[RPT][VW];
-  T own[(kAlpha && !OS) ? RPT : 1][VW];
+  T own[(kAlpha && !OS && !kSym) ? RPT : 1][VW];
 #pragma unroll
   for (int r = 0; r < RPT; r++) {
 #pragma unroll
     for (int i = 0; i < VW; i++) {
       acc[r][i] = T(0);
-      if (kAlpha && !OS) own[r][i] = T(0);
+      if (kAlpha && !OS && !kSym) own[r][i] = T(0);
     }
   }
   const int rlo = grp * RPT;  // this thread's rows: r0 + rlo .. r0 + rlo + RPT
@@ -297,9 +301,14 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       }
 #pragma unroll
       for (int i = 0; i < VW; i++) {
-        if (OS) own_s[(r * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
-        else own[r][i] = xo.v[i];
-        double res = (double)acc[r][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+        double res;
+        if constexpr (kSym) {
+          res = (double)acc[r][i] + 0.5 * (((double)hv.v[i] + hshift) * (double)xo.v[i]);
+        } else {
+          if (OS) own_s[(r * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
+          else own[r][i] = xo.v[i];
+          res = (double)acc[r][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+        }
         if (a.accumulate) res += (double)ov.v[i];
         ov.v[i] = (T)res;
       }
@@ -312,6 +321,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       }
     }
   }
+  if constexpr (kSym) return;  // B only: no C^T
   // transposed write-out: column c gets this thread's rows contiguous (index c * nrows + r), as
   // 16-byte accesses when the block is full and every column starts 16-byte aligned
   constexpr int RW = 16 / sizeof(T);
@@ -484,7 +494,7 @@ int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y) {
   return SBD_TPB_OK;
 }
 
-template <typename T, bool kAlpha, int G, int M, bool OS = false>
+template <typename T, bool kAlpha, int G, int M, bool OS = false, bool kSym = false>
 int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
   constexpr int VW = 16 / sizeof(T);
   constexpr int W = (kBlkThreads / G) * VW;
@@ -499,7 +509,8 @@ int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out,
   const bool vec = (ba.ncols % VW) == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
                    (reinterpret_cast<uintptr_t>(out) % 16) == 0 &&
                    (!XT || (reinterpret_cast<uintptr_t>(XT) % 16) == 0);
-  auto kern = vec ? sigma_block_kernel<T, kAlpha, true, G, M, OS> : sigma_block_kernel<T, kAlpha, false, G, M, OS>;
+  auto kern = vec ? sigma_block_kernel<T, kAlpha, true, G, M, OS, kSym>
+                  : sigma_block_kernel<T, kAlpha, false, G, M, OS, kSym>;
   TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
   TPB_LAUNCHED(h);
@@ -520,6 +531,14 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   } else {
     return launch_block_cfg<T, kAlpha, 2, 9>(h, ba, X, out, XT);
   }
+}
+
+// The symmetric alpha pass: no C^T and no values kept for it, so one CTA per SM more than the
+// alpha pass of the general sigma fits without spills (FP32 8 and FP64 9 spill).
+template <typename T>
+int launch_block_sym(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out) {
+  if constexpr (sizeof(T) == 4) return launch_block_cfg<T, true, 2, 7, false, true>(h, ba, X, out, nullptr);
+  else return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
 }
 
 // Most entries of any kBlkRows-row block of a CSR table of n rows (shared-memory staging size).
@@ -745,6 +764,63 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
   TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
   return SBD_TPB_OK;
 }
+
+// sigma = (H - shift) C for an exchange-symmetric C (C = C^T, alpha strings = beta strings): the
+// symmetric alpha pass writes B = (H_ii - shift) C / 2 + sum_Ja H_a(Ia, Ja) C[Ja, Ib], sym_add
+// forms B + B^T in place (the beta part of sigma is the transpose of the alpha part, and the
+// diagonal halves add back), then the alpha-beta term adds in as in sigma_sep_shift.  One
+// gathering pass instead of two and no C^T.  The result is exact up to rounding only when C is
+// symmetric; the caller guarantees that (Davidson with the exchange-symmetry projection).
+template <typename T>
+int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift) {
+  const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
+  if (na != nb || h->astr != h->bstr)
+    return fail(SBD_TPB_ERR_STATE, "symmetric sigma needs identical alpha and beta strings");
+  const bool dense_ab = h->ab.enabled && sizeof(T) == 4 && h->ab.tc_ready;
+  TPB_CHECK(prepare_sigma_meta(h, !dense_ab));
+  TPB_CHECK(build_coulomb_table(h, h->pa, h->d_bstr, nb));
+  BlockArgs ba{};
+  ba.s_off = h->ta_s.off;
+  ba.s_ket = h->ta_s.ket;
+  ba.s_val = h->pa.s_val;
+  ba.s_valf = h->pa.s_valf;
+  ba.s_pair = h->pa.s_pair;
+  ba.d_off = h->ta_d.off;
+  ba.d_ket = h->ta_d.ket;
+  ba.d_val = h->pa.d_val;
+  ba.d_valf = h->pa.d_valf;
+  ba.col_str = h->d_bstr;
+  ba.jtab = h->pa.jtab;
+  ba.pmap = h->pa.pmap;
+  ba.vd = h->d_vd;
+  ba.L = h->L;
+  ba.nrows = na;
+  ba.ncols = nb;
+  ba.max_d = h->blk_max[0];
+  ba.max_s = h->blk_max[1];
+  ba.hii = h->d_hii;
+  ba.hii32 = h->d_hii32;
+  ba.core_shift = sizeof(T) == 8 ? shift : h->h00 - shift;
+  ba.accumulate = 0;
+  ba.do_ab = 0;
+  TPB_CUDA(cudaEventRecord(h->ev0, h->stream));
+  TPB_CHECK(launch_block_sym<T>(h, ba, C, sigma));
+  TPB_CUDA(cudaEventRecord(h->ev_k[0], h->stream));
+  TPB_CHECK(sym_add<T>(h, sigma));
+  TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
+  if (dense_ab) {
+    TPB_CHECK(ab_dense_apply<T>(h, C, sigma));
+  } else {
+    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma));
+  }
+  TPB_CUDA(cudaEventRecord(h->ev_k[2], h->stream));
+  h->sigma_kernels = 3;
+  TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
+  return SBD_TPB_OK;
+}
+
+template int sigma_sep_sym<double>(sbd_tpb_handle *, const double *, double *, double);
+template int sigma_sep_sym<float>(sbd_tpb_handle *, const float *, float *, double);
 
 // Same two passes with a caller-provided C^T buffer and the alpha-beta terms always evaluated by
 // the direct loop of the alpha pass: needs no device memory beyond C, sigma and CT.

@@ -223,6 +223,10 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
 // sigma (+)= H C with a caller-provided C^T buffer of ndet elements; no device allocation
 template <typename T>
 int sigma_sep_given_ct(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, T *CT);
+// sigma = (H - shift) C for C = C^T over identical alpha and beta strings: one gathering pass and
+// an in-place B + B^T (see sigma.cu)
+template <typename T>
+int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift);
 // per-block table sizes of the sigma launches, read back once per table build (blk_max, blk_for)
 int prepare_block_sizes(sbd_tpb_handle *h);
 int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y);

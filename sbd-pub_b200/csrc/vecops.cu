@@ -261,7 +261,8 @@ __global__ void axpby_kernel(const T *__restrict__ x, T *__restrict__ y, double 
 constexpr int kSymTile = 32;
 constexpr int kSymBlocksPerSm = 16;
 
-template <typename T, int VW>
+// kAvg false: t <- t + t^T (the symmetric sigma's B + B^T), no norm.
+template <typename T, int VW, bool kAvg = true>
 __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint32_t nb, double *partials) {
   constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;  // threads per tile row, row step
   __shared__ T A[TS][TS + 1], B[TS][TS + 1];
@@ -305,11 +306,15 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint
       const uint32_t i = bi * TS + r, j = bj * TS + cx;
       T v[VW];
 #pragma unroll
-      for (int l = 0; l < VW; l++) v[l] = (T)(((double)A[r][cx + l] + (double)B[cx + l][r]) * 0.5);
+      for (int l = 0; l < VW; l++)
+        v[l] = kAvg ? (T)(((double)A[r][cx + l] + (double)B[cx + l][r]) * 0.5)
+                    : (T)((double)A[r][cx + l] + (double)B[cx + l][r]);
       if (i < nb && j < nb) {
         stv<T, VW>(t + (size_t)i * nb + j, v);
+        if (kAvg) {
 #pragma unroll
-        for (int l = 0; l < VW; l++) acc += mult * (double)v[l] * (double)v[l];
+          for (int l = 0; l < VW; l++) acc += mult * (double)v[l] * (double)v[l];
+        }
       }
     }
     if (bi != bj) {
@@ -318,13 +323,17 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint
         const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
         T v[VW];
 #pragma unroll
-        for (int l = 0; l < VW; l++) v[l] = (T)(((double)A[cx + l][r] + (double)B[r][cx + l]) * 0.5);
+        for (int l = 0; l < VW; l++)
+          v[l] = kAvg ? (T)(((double)A[cx + l][r] + (double)B[r][cx + l]) * 0.5)
+                      : (T)((double)A[cx + l][r] + (double)B[r][cx + l]);
         if (i2 < nb && j2 < nb) stv<T, VW>(t + (size_t)i2 * nb + j2, v);
       }
     }
   }
-  double v[1] = {acc};
-  block_reduce_store<1>(v, 1, partials, gridDim.x);
+  if (kAvg) {
+    double v[1] = {acc};
+    block_reduce_store<1>(v, 1, partials, gridDim.x);
+  }
 }
 
 }  // namespace
@@ -511,6 +520,19 @@ int symmetrize(sbd_tpb_handle *h, T *t, double *tt) {
 }
 
 template <typename T>
+int sym_add(sbd_tpb_handle *h, T *x) {
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = h->num_sms * kSymBlocksPerSm;
+  constexpr int VW = 16 / sizeof(T);
+  if (nb % VW == 0 && reinterpret_cast<uintptr_t>(x) % 16 == 0)
+    symmetrize_kernel<T, VW, false><<<nblk, 256, 0, h->stream>>>(x, nb, nullptr);
+  else
+    symmetrize_kernel<T, 1, false><<<nblk, 256, 0, h->stream>>>(x, nb, nullptr);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+template <typename T>
 int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n) {
   scale_kernel<T><<<vec_blocks(h), kVecThreads, 0, h->stream>>>(x, a, n);
   TPB_LAUNCHED(h);
@@ -531,6 +553,8 @@ int axpby(sbd_tpb_handle *h, const T *x, T *y, double a, double b, size_t n) {
   return SBD_TPB_OK;
 }
 
+template int sym_add<double>(sbd_tpb_handle *, double *);
+template int sym_add<float>(sbd_tpb_handle *, float *);
 template int multi_dot<double>(sbd_tpb_handle *, const double *const *, int, const double *,
                                size_t, double *);
 template int multi_dot<float>(sbd_tpb_handle *, const float *const *, int, const float *, size_t,

@@ -42,6 +42,9 @@ int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n);
 // t <- (t + t^T)/2 over the square (alpha = beta strings) determinant matrix; tt = new t.t
 template <typename T>
 int symmetrize(sbd_tpb_handle *h, T *t, double *tt);
+// x <- x + x^T over the square determinant matrix (in place, no reduction)
+template <typename T>
+int sym_add(sbd_tpb_handle *h, T *x);
 
 // The same passes without a host round trip: each reduces into slots of a small device array
 // (kScalarSlots doubles), read back together by fetch_scalars (one stream synchronisation).

@@ -257,6 +257,13 @@ class Handle:
         _check(lib().sbd_tpb_diagonal(self.h, out.ctypes.data, HOST))
         return out
 
+    def diagonal_device(self):
+        """H_ii as a torch float64 CUDA tensor on the handle's device (sbd_tpb_diagonal, device copy)."""
+        import torch
+        out = torch.empty(self.problem.ndet, dtype=torch.float64, device=f"cuda:{self.device}")
+        _check(lib().sbd_tpb_diagonal(self.h, out.data_ptr(), DEVICE))
+        return out
+
     def sigma(self, C_, out=None, accumulate: bool = False):
         """sigma (+)= H C for numpy (host) or torch CUDA (device) vectors, float64 or float32."""
         dev = not isinstance(C_, np.ndarray)
@@ -287,11 +294,13 @@ class Handle:
             raise TpbError(ERR_INVALID, "sigma input and output must be distinct buffers")
         return 1 if x.dtype == torch.float32 else 0
 
-    def sigma_device(self, x, y, accumulate=False, separated=True):
-        """sigma on torch CUDA tensors; separated=True keeps the library's internal convention."""
+    def sigma_device(self, x, y, accumulate=False, separated=True, symmetric=False):
+        """sigma on torch CUDA tensors; separated=True keeps the library's internal convention;
+        symmetric=True (separated, exchange-symmetric x over identical string lists) takes the
+        one-pass form (convention 2)."""
         dt = self._device_pair(x, y)
-        _check(lib().sbd_tpb_sigma_device(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate),
-                                          1 if separated else 0))
+        conv = 2 if symmetric else (1 if separated else 0)
+        _check(lib().sbd_tpb_sigma_device(self.h, x.data_ptr(), y.data_ptr(), dt, int(accumulate), conv))
         return y
 
     def sigma_noalloc(self, x, y, accumulate=False):
