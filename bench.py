@@ -68,6 +68,10 @@ def parse():
                     help="skip the learned-vs-diagonal solves on the 28-orbital problem")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass")
     ap.add_argument("--no-carryover", action="store_true", help="skip the carry-over measurement")
+    ap.add_argument("--accuracy-report", action="store_true",
+                    help="only solve every workload config (12-orbital FCI, 24/32/28/36-orbital selected "
+                         "CI) in FP64, mixed and mixed + learned and print one JSON line of the energy, "
+                         "FP64-residual and RDM errors against the FP64 path")
     ap.add_argument("--davidson-cycle", action="store_true",
                     help="only run one Davidson cycle (8 sigma steps, final FP64 sigma) on the workload "
                          "and print its time; the command the Davidson launch-list profile is taken on")
@@ -88,6 +92,65 @@ def run_davidson_cycle(args, local):
                       "seconds": dt, "ms_per_step": 1e3 * dt / max(1, r["iterations"]),
                       "energy": r["energy"]}), flush=True)
     h.close()
+
+
+# Solver settings per workload for the accuracy report: FP64 reference tolerance, the compared
+# solves' tolerance, subspace sizes (FP64 / mixed; the 1.6e9-determinant FP64 run is limited to 4
+# vectors by 180 GB of HBM).  The 12-orbital FCI is solved to |r| < 1e-8 in FP64 (its benchmark
+# setting); FP32 vectors cannot resolve that, so its mixed solves stop at 1e-5.
+ACCURACY = [
+    ("fci12", 1e-8, 1e-5, 10, 10),
+    ("sci24", 1e-6, 1e-4, 8, 8),
+    ("sci32", 1e-6, 1e-4, 8, 8),
+    ("sci28", 1e-6, 1e-4, 8, 8),
+    ("sci36", 1e-6, 1e-4, 4, 6),
+]
+
+
+def accuracy_report(args, local):
+    """Energy, FP64 residual and 1/2-RDM errors of the mixed-precision and mixed + learned solves
+    against the plain FP64 solve, every workload config, from the HF start; RDMs from the final
+    vectors (the library's FP64 RDM kernels), the residual |HW - EW| from the final FP64 sigma."""
+    import torch
+
+    import sbd_tpb
+    import synth
+    torch.cuda.set_device(local)
+    pc, train = train_preconditioner(local)
+    out = {"learned_training": train}
+    for name, eps64, eps, nb64, nbm in ACCURACY:
+        h = sbd_tpb.Handle(local)
+        h.set_problem(synth.make_problem(name))
+        runs = {}
+        for tag, prec, pre, e_, nb_ in (("fp64", sbd_tpb.FP64, sbd_tpb.PRECOND_DIAGONAL, eps64, nb64),
+                                        ("mixed", sbd_tpb.MIXED, sbd_tpb.PRECOND_DIAGONAL, eps, nbm),
+                                        ("mixed_learned", sbd_tpb.MIXED, sbd_tpb.PRECOND_LEARNED, eps, nbm)):
+            if pre == sbd_tpb.PRECOND_LEARNED:
+                h.set_preconditioner(pc)
+            t0 = time.perf_counter()
+            r = h.davidson(sbd_tpb.default_params(max_it=60, max_nb=nb_, eps=e_, precision=prec,
+                                                  preconditioner=pre), want_vector=False, want_rdm=True)
+            runs[tag] = dict(r, seconds_wall=time.perf_counter() - t0)
+            h.set_preconditioner(None)
+            h.free_vectors()
+        ref = runs["fp64"]
+        rec = {"determinants": h.problem.ndet, "fp64": {"energy": ref["energy"], "residual": ref["residual"],
+                                                         "sigma_steps": ref["iterations"],
+                                                         "seconds": ref["seconds_wall"], "eps": eps64,
+                                                         "subspace": nb64}}
+        for tag in ("mixed", "mixed_learned"):
+            r = runs[tag]
+            rec[tag] = {"energy": r["energy"], "abs_energy_error": abs(r["energy"] - ref["energy"]),
+                        "fp64_residual": r["residual"], "sigma_steps": r["iterations"],
+                        "learned_steps": r["learned_steps"], "fallback_steps": r["fallback_steps"],
+                        "seconds": r["seconds_wall"], "eps": eps, "subspace": nbm,
+                        "max_abs_1rdm_error": float(np.max(np.abs(r["one"] - ref["one"]))),
+                        "max_abs_2rdm_error": float(np.max(np.abs(r["two"] - ref["two"])))}
+        out[name] = rec
+        h.close()
+        torch.cuda.empty_cache()
+    pc.close()
+    print(json.dumps({"accuracy_report": out}), flush=True)
 
 
 def peaks():
@@ -646,6 +709,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.accuracy_report:
+            accuracy_report(args, local)
         elif args.davidson_cycle:
             run_davidson_cycle(args, local)
         else:

@@ -6,13 +6,14 @@
 // sort_bitarray, bdet = adet) through both sbd::tpb::diag (tpb/sbdiag.h:139-151, the reference on the
 // host) and sbd_b200::diag (the library on the GPU) with the same settings.  Prints one line of
 // key=value pairs: the two energies, the largest differences of density, 1-RDM and 2-RDM entries,
-// and whether the carry-over strings are equal.
+// and whether the carry-over strings are equal (as sets, and in the same order).
 // Usage: binding_check --fcidump F --adetfile A [--iteration I] [--block B] [--tolerance T]
 //                      [--rdm] [--carryover_type K --carryover_threshold X]
 //                      [--loadname NAME] [--savename NAME] [--skip_reference]
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <deque>
 #include <iostream>
 #include <string>
@@ -95,12 +96,21 @@ int main(int argc, char **argv) {
     return 3;
   }
   const double t_b200 = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+  // carry-over strings: in the same order, and as sets (strings of equal weight, e.g. related by
+  // the molecule's spatial symmetry, may be ordered differently by rounding-level differences of
+  // the two vectors; the next load of the strings sorts them)
+  auto sorted = [](std::vector<std::vector<size_t>> v) {
+    std::sort(v.begin(), v.end());
+    return v;
+  };
+  const int co_seq = (int)(ca_ref == ca_b200 && cb_ref == cb_b200);
+  const int co_set = (int)(sorted(ca_ref) == sorted(ca_b200) && sorted(cb_ref) == sorted(cb_b200));
   std::printf("e_ref=%.15f e_b200=%.15f density_diff=%.3e rdm1_diff=%.3e rdm2_diff=%.3e "
-              "co_equal=%d co_a=%zu co_b=%zu t_ref=%.3f t_b200=%.3f\n",
+              "co_equal=%d co_same_order=%d co_a=%zu co_b=%zu co_a_ref=%zu co_b_ref=%zu t_ref=%.3f t_b200=%.3f\n",
               e_ref, e_b200, skip_reference ? 0.0 : max_diff(d_ref, d_b200),
               s.do_rdm && !skip_reference ? max_diff(one_ref, one_b200) : 0.0,
-              s.do_rdm && !skip_reference ? max_diff(two_ref, two_b200) : 0.0,
-              (int)(ca_ref == ca_b200 && cb_ref == cb_b200), ca_b200.size(), cb_b200.size(), t_ref, t_b200);
+              s.do_rdm && !skip_reference ? max_diff(two_ref, two_b200) : 0.0, co_set, co_seq,
+              ca_b200.size(), cb_b200.size(), ca_ref.size(), cb_ref.size(), t_ref, t_b200);
   MPI_Finalize();
   return 0;
 }

@@ -5,8 +5,10 @@
 // (k+1)x(k+1) projection, W = sum U_k0 C_k, R = E0 W - H W, convergence when |R| < eps, diagonal
 // correction t = R / (E0 - H_ii) with the 1e-12 regularisation, Gram-Schmidt against the subspace,
 // restart from W after max_nb steps, and the max_time guard.  The small eigenproblem is solved on
-// the host with a cyclic Jacobi method, eigenvalues sorted ascending (the reference calls LAPACK
-// dsyev, framework/hp_numeric.h:500-520, which also returns them ascending).
+// the device (rr_solve: the projected matrix kept in HBM, cyclic Jacobi on one warp, eigenvalues
+// sorted ascending; the reference calls LAPACK dsyev on the host, framework/hp_numeric.h:500-520,
+// which also returns them ascending), so a step synchronises with the host once, to read its
+// scalars for the convergence test.
 //
 // Vectors live in HBM in the separated sign convention.  The FP64 path keeps everything in
 // double.  The mixed path stores C/HC/W/t in FP32, computes sigma of (H - s) with s = H_00 so the
@@ -32,61 +34,11 @@
 namespace sbdtpb {
 namespace {
 
-// Cyclic Jacobi eigen-solver; A is n x n column-major with leading dimension lda (only the
-// leading n x n block is read).  On return V holds eigenvectors (columns), E eigenvalues sorted
-// ascending.
-void jacobi_eigen(int n, const double *A, int lda, std::vector<double> &E, std::vector<double> &V) {
-  std::vector<double> M((size_t)n * n);
-  V.assign((size_t)n * n, 0.0);
-  for (int j = 0; j < n; j++)
-    for (int i = 0; i < n; i++) M[i + (size_t)n * j] = A[i + (size_t)lda * j];
-  for (int i = 0; i < n; i++) V[i + (size_t)n * i] = 1.0;
-  for (int sweep = 0; sweep < 100; sweep++) {
-    double off = 0.0, diag = 0.0;
-    for (int j = 0; j < n; j++) {
-      diag += M[j + (size_t)n * j] * M[j + (size_t)n * j];
-      for (int i = 0; i < j; i++) off += M[i + (size_t)n * j] * M[i + (size_t)n * j];
-    }
-    if (off <= 1e-32 * (diag + 1e-300)) break;
-    for (int p = 0; p < n; p++) {
-      for (int q = p + 1; q < n; q++) {
-        const double apq = M[p + (size_t)n * q];
-        if (std::fabs(apq) < 1e-300) continue;
-        const double app = M[p + (size_t)n * p], aqq = M[q + (size_t)n * q];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < n; k++) {
-          const double mkp = M[k + (size_t)n * p], mkq = M[k + (size_t)n * q];
-          M[k + (size_t)n * p] = c * mkp - s * mkq;
-          M[k + (size_t)n * q] = s * mkp + c * mkq;
-        }
-        for (int k = 0; k < n; k++) {
-          const double mpk = M[p + (size_t)n * k], mqk = M[q + (size_t)n * k];
-          M[p + (size_t)n * k] = c * mpk - s * mqk;
-          M[q + (size_t)n * k] = s * mpk + c * mqk;
-        }
-        for (int k = 0; k < n; k++) {
-          const double vkp = V[k + (size_t)n * p], vkq = V[k + (size_t)n * q];
-          V[k + (size_t)n * p] = c * vkp - s * vkq;
-          V[k + (size_t)n * q] = s * vkp + c * vkq;
-        }
-      }
-    }
-  }
-  std::vector<int> ord(n);
-  for (int i = 0; i < n; i++) ord[i] = i;
-  for (int i = 0; i < n; i++)
-    for (int j = i + 1; j < n; j++)
-      if (M[ord[j] + (size_t)n * ord[j]] < M[ord[i] + (size_t)n * ord[i]]) std::swap(ord[i], ord[j]);
-  std::vector<double> Vs((size_t)n * n);
-  E.resize(n);
-  for (int k = 0; k < n; k++) {
-    E[k] = M[ord[k] + (size_t)n * ord[k]];
-    for (int i = 0; i < n; i++) Vs[i + (size_t)n * k] = V[i + (size_t)n * ord[k]];
-  }
-  V.swap(Vs);
-}
+// Reduction slots of one Davidson step (device array of kScalarSlots doubles read back together):
+// [0, ib+4) residual pass (W.W, r.r, S_k.t, t.t), 20 t.t after the symmetric projection,
+// [24, 24+ib+2) first Gram-Schmidt round (t.t, S_k.t), 41 t.t after the second round (0 when the
+// device skipped it), [44, 44+ib+1) overlaps S_k . sigma(S_ib), [60, 64) the lowest Ritz values.
+constexpr int kSymSlot = 20, kCgsSlot = 24, kCgs2Slot = 41, kOvSlot = 44, kEigSlot = 60;
 
 template <typename T>
 int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, double shift,
@@ -131,7 +83,6 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
     f[0] = 1.0 / std::sqrt(nrm);
   }
 
-  std::vector<double> Hs((size_t)nb * nb, 0.0), E, U;
   std::vector<double> out(kMaxVec + 2), dots(kMaxVec + 2);
   std::vector<double> step_times;
   double norm_R = 0.0, ww = 1.0;
@@ -182,21 +133,20 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       nsigma++;
       std::vector<const T *> cp(ib + 1);
       for (int k = 0; k <= ib; k++) cp[k] = S[k].p;
-      TPB_CHECK(multi_dot<T>(h, cp.data(), ib + 1, HS[ib].p, n, out.data()));
-      for (int k = 0; k <= ib; k++) {
-        const double v = f[k] * f[ib] * out[k];
-        Hs[k + (size_t)nb * ib] = v;
-        Hs[ib + (size_t)nb * k] = v;
-      }
-      jacobi_eigen(ib + 1, Hs.data(), nb, E, U);
+      // the new column of the projected matrix and its Rayleigh-Ritz solve stay on the device;
+      // the residual kernel reads the Ritz coefficients from there
+      ScaleArray fa;
+      for (int k = 0; k < kMaxSub; k++) fa.v[k] = k <= ib ? f[k] : 0.0;
+      TPB_CHECK(multi_dot_async<T>(h, cp.data(), ib + 1, HS[ib].p, n, kOvSlot));
+      TPB_CHECK(rr_solve(h, ib, fa, kOvSlot, kEigSlot));
       for (int k = 0; k < kMaxVec; k++) {
         ra.C.p[k] = k <= ib ? S[k].p : nullptr;
         ra.HC.p[k] = k <= ib ? HS[k].p : nullptr;
       }
-      for (int k = 0; k < kMaxSub; k++) ra.u[k] = k <= ib ? U[k] * f[k] : 0.0;
+      ra.u_dev = rr_u(h);
+      ra.e_dev = rr_e(h);
+      ra.shift = shift;
       ra.m = ib + 1;
-      ra.e_shifted = E[0];
-      ra.e0 = E[0] + shift;
       // FP32 vectors: the correction's denominator from H_ii - H_00 in FP32 (half the bytes of the
       // FP64 diagonal; its 1e-7 relative rounding is far below what a preconditioner needs)
       ra.hii = h->d_hii;
@@ -207,32 +157,36 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       ra.W = last ? Wv.p : nullptr;
       T *tnext = last ? nullptr : S[ib + 1].p;
       ra.t = tnext;
-      // Fast path: residual, symmetric projection and the first Gram-Schmidt round go back to back
-      // (the CGS kernel reads the overlaps from device memory) and their scalars come back with
-      // one synchronisation.  If this step turns out converged, the extra work on t is discarded.
+      // Fast path: residual, symmetric projection and both Gram-Schmidt rounds (the second one
+      // decided on the device) go back to back, and the step's scalars come back with its one
+      // synchronisation.  If this step turns out converged, the extra work on t is discarded.
       const bool fast = !rec && !last && !(learned && cycle_mode == 1);
       double t0_fast = 0.0, tt_fast = 0.0;
+      TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
+      std::vector<double> coef(ib + 1);
+      for (int k = 0; k <= ib; k++) coef[k] = f[k] * f[k];
       if (fast) {
-        constexpr int kSymSlot = 20, kCgsSlot = 24;
-        TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
         if (sym) TPB_CHECK(symmetrize_async<T>(h, tnext, kSymSlot));
-        std::vector<double> coef(ib + 1);
-        for (int k = 0; k <= ib; k++) coef[k] = f[k] * f[k];
+        const int t0_slot = sym ? kSymSlot : 2 + ib + 1;
         TPB_CHECK(cgs_update_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, n, 1, kCgsSlot));
-        const double *sc = fetch_scalars(h, kCgsSlot + ib + 2);
-        if (!sc) return SBD_TPB_ERR_CUDA;
-        for (int k = 0; k < ib + 4; k++) out[k] = sc[k];
-        t0_fast = sym ? sc[kSymSlot] : sc[2 + ib + 1];
-        tt_fast = sc[kCgsSlot];
-        for (int k = 0; k <= ib; k++) dots[1 + k] = sc[kCgsSlot + 1 + k];
-      } else {
-        TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+        TPB_CHECK(cgs_second_round_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, n, t0_slot,
+                                            kCgsSlot, kCgs2Slot));
       }
+      const double *sc = fetch_scalars(h, kScalarSlots);
+      if (!sc) return SBD_TPB_ERR_CUDA;
+      for (int k = 0; k < ib + 4; k++) out[k] = sc[k];  // W.W, r.r, S_k.t, t.t
+      if (fast) {
+        t0_fast = sym ? sc[kSymSlot] : sc[2 + ib + 1];
+        const double tt1 = sc[kCgsSlot];
+        tt_fast = tt1 < 0.5 * t0_fast ? sc[kCgs2Slot] : tt1;
+      }
+      double eig[4];
+      for (int p = 0; p < 4; p++) eig[p] = sc[kEigSlot + p] + shift;
       w_current = last;
       m_last = ib + 1;
       ww = out[0];
       norm_R = std::sqrt(out[1] / ww);
-      energy = ra.e0;
+      energy = eig[0];
       bool recording = false;
       if (rec && !last && (int)rec->d.size() < rec->max_steps) {
         // keep d_k, E_k, |r_k| and the step's basis for training pairs (dperp after Gram-Schmidt)
@@ -251,7 +205,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         rec->owned.push_back(dk);
         rec->d.push_back(dk);
         TPB_CHECK((convert_vec<T, float>(h, tnext, dk, n)));
-        rec->e0.push_back(ra.e0);
+        rec->e0.push_back(energy);
         rec->rnorm.push_back(std::sqrt(out[1]));
         rec->basis.push_back(rec_cycle);
       }
@@ -274,7 +228,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       prev_norm = norm_R;
       if (prm->verbose) {
         std::printf(" Davidson iteration %d.%d (tol=%.16g):", it, ib, norm_R);
-        for (int p = 0; p < std::min(ib + 1, 4); p++) std::printf(" %.16g", E[p] + shift);
+        for (int p = 0; p < std::min(ib + 1, 4); p++) std::printf(" %.16g", eig[p]);
         std::printf("\n");
         std::fflush(stdout);
       }
@@ -284,7 +238,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         break;
       }
       if (use_learned)
-        TPB_CHECK(precond_apply<T>(h, learned, tnext, ra.e0, std::sqrt(out[1]), out[2 + ib + 1]));
+        TPB_CHECK(precond_apply<T>(h, learned, tnext, energy, std::sqrt(out[1]), out[2 + ib + 1]));
       if (sym && !last && !fast) {
         // the S_k are exactly symmetric, so S_k.t is unchanged by the projection; only t.t is
         TPB_CHECK(symmetrize<T>(h, tnext, &out[2 + ib + 1]));
@@ -305,16 +259,16 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         // subspace to working precision).
         double t0 = t0_fast, tt = tt_fast;
         std::vector<double> o(ib + 1);
-        if (!fast) {
+        if (!fast) {  // (the fast path ran both rounds on the device)
           t0 = out[2 + ib + 1];
           for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * out[2 + k];
           TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 1, dots.data()));
           tt = dots[0];
-        }
-        if (tt < 0.5 * t0) {
-          for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * dots[1 + k];
-          TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 0, dots.data()));
-          tt = dots[0];
+          if (tt < 0.5 * t0) {
+            for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * dots[1 + k];
+            TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 0, dots.data()));
+            tt = dots[0];
+          }
         }
         if (!(tt > 0.0)) {
           // the correction lies in the subspace: nothing left to add
@@ -332,8 +286,9 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
           rec_cycle.push_back((int)rec->vec.size() - 1);
         }
       }
-      // max_time guard (tpb/davidson.h:887-913): stop when the next step would overrun
-      TPB_CUDA(cudaStreamSynchronize(h->stream));
+      // max_time guard (tpb/davidson.h:887-913): stop when the next step would overrun (after the
+      // fast path the stream is already idle)
+      if (!fast) TPB_CUDA(cudaStreamSynchronize(h->stream));
       const auto s1 = std::chrono::steady_clock::now();
       step_times.push_back(std::chrono::duration<double>(s1 - s0).count());
       double avg = 0.0;

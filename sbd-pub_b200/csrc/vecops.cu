@@ -170,6 +170,13 @@ struct ResidualBody {
 
 template <typename T, int M>
 __global__ void __launch_bounds__(kVecThreads) residual_kernel(ResidualArgs<T> a, size_t n, double *partials) {
+  if (a.u_dev) {
+    // Ritz coefficients and value of the device Rayleigh-Ritz solve
+#pragma unroll
+    for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
+    a.e_shifted = __ldg(&a.e_dev[0]);
+    a.e0 = a.e_shifted + a.shift;
+  }
   double acc[M + 3];
 #pragma unroll
   for (int j = 0; j < M + 3; j++) acc[j] = 0.0;
@@ -213,13 +220,21 @@ struct CgsBody {
 };
 
 // o_k = co.v[k] * (ov ? ov[k] : 1): the overlaps may come straight from a device reduction
+// pred (may be null): run only when pred[1] < 0.5 * pred[0] (the second Gram-Schmidt round, decided
+// on the device from the first round's |t|^2 before and after); a skipped launch writes zero
+// partials (its reduction is then 0 and nothing else changes)
 template <typename T, int M, bool kDots>
 __global__ void __launch_bounds__(kVecThreads)
     cgs_update_kernel(VecPtrs<T> C, CoefArray co, const double *__restrict__ ov, T *__restrict__ t, size_t n,
-                      double *partials) {
+                      double *partials, const double *__restrict__ pred0 = nullptr,
+                      const double *__restrict__ pred1 = nullptr) {
   double acc[M + 1];
 #pragma unroll
   for (int j = 0; j < M + 1; j++) acc[j] = 0.0;
+  if (pred0 && !(__ldg(pred1) < 0.5 * __ldg(pred0))) {
+    if (threadIdx.x <= (kDots ? M : 0)) partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = 0.0;
+    return;
+  }
   double o[M];
 #pragma unroll
   for (int k = 0; k < M; k++) o[k] = co.v[k] * (ov ? __ldg(&ov[k]) : 1.0);
@@ -336,6 +351,91 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint
   }
 }
 
+// Rayleigh-Ritz of the Davidson subspace on one warp.  Hs (ld kMaxSub, column-major, persistent
+// across the steps of a cycle) gets column and row ib = f_k f_ib ov_k; the leading n = ib + 1
+// block is diagonalised by cyclic Jacobi rotations in shared memory (each rotation's row and
+// column updates split over the lanes), the eigenvalues sorted ascending as dsyev returns them.
+// Outputs: u[k] = V[k][lowest] * f_k, e[0..n) ascending, eig4[0..3] = the lowest four (0 past n).
+__global__ void __launch_bounds__(32) rr_kernel(double *__restrict__ Hs, const double *__restrict__ ov,
+                                                ScaleArray f, int ib, double *__restrict__ u,
+                                                double *__restrict__ e, double *__restrict__ eig4) {
+  constexpr int S = kMaxSub;
+  __shared__ double M[S][S + 1], V[S][S + 1];
+  __shared__ int ord[S];
+  const int lane = threadIdx.x, n = ib + 1;
+  if (lane <= ib) {
+    const double v = f.v[lane] * f.v[ib] * ov[lane];
+    Hs[lane + S * ib] = v;
+    Hs[ib + S * lane] = v;
+  }
+  __syncwarp();
+  for (int idx = lane; idx < n * n; idx += 32) {
+    const int i = idx % n, j = idx / n;
+    M[i][j] = Hs[i + S * j];
+    V[i][j] = i == j ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0, diag = 0.0;
+    for (int idx = lane; idx < n * n; idx += 32) {
+      const int i = idx % n, j = idx / n;
+      if (i == j) diag += M[i][j] * M[i][j];
+      else if (i < j) off += M[i][j] * M[i][j];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      diag += __shfl_xor_sync(0xffffffffu, diag, o);
+    }
+    if (off <= 1e-32 * (diag + 1e-300)) break;
+    for (int p = 0; p < n; p++) {
+      for (int q = p + 1; q < n; q++) {
+        const double apq = M[p][q];
+        if (fabs(apq) < 1e-300) continue;
+        const double app = M[p][p], aqq = M[q][q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        __syncwarp();
+        if (lane < n) {  // columns p, q
+          const double mkp = M[lane][p], mkq = M[lane][q];
+          M[lane][p] = c * mkp - s * mkq;
+          M[lane][q] = s * mkp + c * mkq;
+        }
+        __syncwarp();
+        if (lane < n) {  // rows p, q
+          const double mpk = M[p][lane], mqk = M[q][lane];
+          M[p][lane] = c * mpk - s * mqk;
+          M[q][lane] = s * mpk + c * mqk;
+        } else if (lane >= 16 && lane - 16 < n) {  // eigenvectors
+          const int k = lane - 16;
+          const double vkp = V[k][p], vkq = V[k][q];
+          V[k][p] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < n; i++) ord[i] = i;
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++)
+        if (M[ord[j]][ord[j]] < M[ord[i]][ord[i]]) {
+          const int x = ord[i];
+          ord[i] = ord[j];
+          ord[j] = x;
+        }
+  }
+  __syncwarp();
+  if (lane < n) {
+    e[lane] = M[ord[lane]][ord[lane]];
+    u[lane] = V[lane][ord[0]] * f.v[lane];
+  }
+  if (lane < 4) eig4[lane] = lane < n ? M[ord[lane]][ord[lane]] : 0.0;
+}
+
 }  // namespace
 
 int ensure_partials(sbd_tpb_handle *h, size_t n) {
@@ -351,10 +451,27 @@ int ensure_partials(sbd_tpb_handle *h, size_t n) {
 int vec_blocks(sbd_tpb_handle *h) { return h->num_sms * 4; }
 
 // device slots for reductions whose results are read back together (pinned host mirror)
+// (with them the Rayleigh-Ritz state: the projected matrix, u and the eigenvalues)
+constexpr int kRrDoubles = kMaxSub * kMaxSub + 2 * kMaxSub;
 static int ensure_scalars(sbd_tpb_handle *h) {
   if (h->d_scal) return SBD_TPB_OK;
-  TPB_CUDA(cudaMalloc(&h->d_scal, sizeof(double) * kScalarSlots));
+  TPB_CUDA(cudaMalloc(&h->d_scal, sizeof(double) * (kScalarSlots + kRrDoubles)));
+  TPB_CUDA(cudaMemset(h->d_scal, 0, sizeof(double) * (kScalarSlots + kRrDoubles)));
   TPB_CUDA(cudaMallocHost(&h->h_scal, sizeof(double) * kScalarSlots));
+  return SBD_TPB_OK;
+}
+
+static double *rr_base(sbd_tpb_handle *h) { return h->d_scal + kScalarSlots; }
+const double *rr_u(sbd_tpb_handle *h) { return rr_base(h) + kMaxSub * kMaxSub; }
+const double *rr_e(sbd_tpb_handle *h) { return rr_base(h) + kMaxSub * kMaxSub + kMaxSub; }
+
+int rr_solve(sbd_tpb_handle *h, int ib, const ScaleArray &f, int ov_slot, int eig_slot) {
+  if (ib < 0 || ib >= kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  double *base = rr_base(h);
+  rr_kernel<<<1, 32, 0, h->stream>>>(base, h->d_scal + ov_slot, f, ib, base + kMaxSub * kMaxSub,
+                                     base + kMaxSub * kMaxSub + kMaxSub, h->d_scal + eig_slot);
+  TPB_LAUNCHED(h);
   return SBD_TPB_OK;
 }
 
@@ -477,6 +594,45 @@ int cgs_update_async(sbd_tpb_handle *h, const T *const *C, int m, const double *
   return reduce_into(h, want_dots ? 1 + m : 1, h->d_scal + slot);
 }
 
+template <typename T>
+int multi_dot_async(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n, int slot) {
+  if (k < 1 || k > kMaxVec) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  const int nb = vec_blocks(h);
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
+  VecPtrs<T> P;
+  for (int j = 0; j < kMaxVec; j++) P.p[j] = (j < k) ? X[j] : nullptr;
+  TPB_CHECK(dispatch_n<1>(k, [&](auto K) {
+    multi_dot_kernel<T, decltype(K)::value><<<nb, kVecThreads, 0, h->stream>>>(P, y, n, h->d_partials);
+    TPB_LAUNCHED(h);
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, k, h->d_scal + slot);
+}
+
+template <typename T>
+int cgs_second_round_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                           size_t n, int t0_slot, int tt_slot, int slot) {
+  if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  const int nb = vec_blocks(h);
+  TPB_CHECK(ensure_partials(h, (size_t)(kMaxVec + 3) * nb + kMaxVec + 3));
+  VecPtrs<T> P;
+  CoefArray co;
+  for (int j = 0; j < kMaxVec; j++) P.p[j] = j < m ? C[j] : nullptr;
+  for (int j = 0; j < kMaxSub; j++) co.v[j] = j < m ? coef[j] : 0.0;
+  TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      cgs_update_kernel<T, M, false><<<nb, kVecThreads, 0, h->stream>>>(
+          P, co, h->d_scal + ov_slot, t, n, h->d_partials, h->d_scal + t0_slot, h->d_scal + tt_slot);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, 1, h->d_scal + slot);
+}
+
 const double *fetch_scalars(sbd_tpb_handle *h, int count) {
   if (ensure_scalars(h) != SBD_TPB_OK) return nullptr;
   if (cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream) !=
@@ -553,6 +709,12 @@ int axpby(sbd_tpb_handle *h, const T *x, T *y, double a, double b, size_t n) {
   return SBD_TPB_OK;
 }
 
+template int multi_dot_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, size_t, int);
+template int multi_dot_async<float>(sbd_tpb_handle *, const float *const *, int, const float *, size_t, int);
+template int cgs_second_round_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, int,
+                                            double *, size_t, int, int, int);
+template int cgs_second_round_async<float>(sbd_tpb_handle *, const float *const *, int, const double *, int,
+                                           float *, size_t, int, int, int);
 template int sym_add<double>(sbd_tpb_handle *, double *);
 template int sym_add<float>(sbd_tpb_handle *, float *);
 template int multi_dot<double>(sbd_tpb_handle *, const double *const *, int, const double *,

@@ -25,6 +25,10 @@ struct ResidualArgs {
   int m;              // subspace size
   double e_shifted;   // Ritz value of (H - shift)
   double e0;          // Ritz value of H
+  // when set, u, e_shifted and e0 = e_shifted + shift are read from the device Rayleigh-Ritz
+  // result instead (rr_solve: u_dev[k], e_dev[0])
+  const double *u_dev = nullptr, *e_dev = nullptr;
+  double shift = 0.0;
   const double *hii;  // FP64 diagonal (FP64 vectors)
   const float *hii32; // H_ii - H_00 in FP32 (FP32 vectors; used with e_shifted = E - H_00)
   T *W;               // Ritz vector out (may be null)
@@ -58,6 +62,28 @@ template <typename T>
 int cgs_update_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
                      size_t n, int want_dots, int slot);
 const double *fetch_scalars(sbd_tpb_handle *h, int count);
+
+// Device Rayleigh-Ritz of the Davidson subspace (replaces the host dsyev of tpb/davidson.h:
+// 770-780).  The projected matrix lives in h->d_rr (kMaxSub x kMaxSub, column-major): rr_solve
+// sets its column/row ib to f_k f_ib ov_k (ov = the overlaps S_k . sigma(S_ib) in device slots
+// ov_slot..), solves the leading (ib+1) x (ib+1) eigenproblem with a cyclic Jacobi method
+// (eigenvalues sorted ascending), and leaves u_k = U_k0 f_k at rr_u(h), the eigenvalues at
+// rr_e(h) and the lowest four in slots eig_slot.. (for the host's convergence and print lines).
+struct ScaleArray {
+  double v[kMaxSub];
+};
+int rr_solve(sbd_tpb_handle *h, int ib, const ScaleArray &f, int ov_slot, int eig_slot);
+const double *rr_u(sbd_tpb_handle *h);
+const double *rr_e(sbd_tpb_handle *h);
+// multi_dot into device slots (no host round trip): slot + j = X_j . y
+template <typename T>
+int multi_dot_async(sbd_tpb_handle *h, const T *const *X, int k, const T *y, size_t n, int slot);
+// second Gram-Schmidt round, run only where the first cancelled more than half of |t|^2: t -=
+// sum_k coef_k ov_k C_k when slot tt_slot < 0.5 * slot t0_slot (both device values); the new
+// t.t goes to slot `slot`, or 0 there when the round is skipped
+template <typename T>
+int cgs_second_round_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                           size_t n, int t0_slot, int tt_slot, int slot);
 template <typename S, typename D>
 int convert_vec(sbd_tpb_handle *h, const S *x, D *y, size_t n);
 template <typename T>

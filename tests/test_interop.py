@@ -103,7 +103,11 @@ def test_binding_matches_reference_diag(tmp_path):
     assert abs(float(kv["e_b200"]) - meta["energy"]) < 1e-8, kv
     assert float(kv["density_diff"]) < 1e-6, kv
     assert float(kv["rdm1_diff"]) < 1e-6 and float(kv["rdm2_diff"]) < 1e-6, kv
+    # the same carry-over strings (as sets: strings of equal weight may be ordered differently by
+    # rounding-level differences of the two vectors, and the next load sorts them)
     assert kv["co_equal"] == "1" and int(kv["co_a"]) > 0, kv
+    print(f"\nbinding vs sbd::tpb::diag: dE {abs(float(kv['e_ref']) - float(kv['e_b200'])):.1e}, carry-over "
+          f"{kv['co_a']}/{kv['co_b']} strings, same order: {kv['co_same_order']}")
 
 
 @needs_ref

@@ -271,7 +271,7 @@ def test_gpu_precond_training_gain(trained):
     lh, dh = pc.evaluate(1)
     print(f"\ntraining pairs: learned/diagonal error {lt / dt:.4f}; held-out (sci24): {lh / dh:.4f}")
     assert lt < 0.95 * dt
-    assert np.isfinite(lh)
+    assert lh < dh  # held-out pairs of another system (never trained on) improve too
 
 
 @pytest.mark.gpu
@@ -297,6 +297,36 @@ def test_gpu_davidson_learned_same_answer(trained):
     # |r| < 1e-5 bounds the energy error by ~|r|^2 / gap
     assert abs(rl["energy"] - r64["energy"]) < 1e-7
     assert abs(rm["energy"] - r64["energy"]) < 1e-6
+    h.close()
+
+
+@pytest.mark.gpu
+def test_gpu_learned_held_out_solver_steps(trained):
+    """Solver steps on a system the network never saw (24 orbitals, 2,000 x 2,000 selected
+    strings), learned against diagonal correction, FP64 and mixed, to |r| < 1e-5.  Printed for the
+    record; asserted: the same energy, and that the per-cycle fallback keeps a learned solve within
+    25 % of the diagonal solve's step count (on these random-integral Hamiltonians the learned
+    correction does not reliably save steps)."""
+    import sbd_tpb
+    import synth
+    h = sbd_tpb.Handle(0)
+    h.set_problem(synth.make_problem("sci24", nstrings=2000))
+    h.set_preconditioner(trained["pc"])
+    res = {}
+    for prec, tag in ((sbd_tpb.FP64, "fp64"), (sbd_tpb.MIXED, "mixed")):
+        for pre, ptag in ((sbd_tpb.PRECOND_DIAGONAL, "diagonal"), (sbd_tpb.PRECOND_LEARNED, "learned")):
+            res[tag, ptag] = h.davidson(sbd_tpb.default_params(max_it=40, max_nb=8, eps=1e-5, precision=prec,
+                                                               preconditioner=pre), want_vector=False)
+    print("\nheld-out sci24 (2000 x 2000) steps to |r| < 1e-5: " + ", ".join(
+        f"{t}/{p} {r['iterations']} ({r['learned_steps']} learned, {r['fallback_steps']} fallbacks)"
+        for (t, p), r in res.items()))
+    e = res["fp64", "diagonal"]["energy"]
+    for (t, p), r in res.items():
+        assert r["converged"], (t, p)
+        assert abs(r["energy"] - e) < 1e-6, (t, p, r["energy"], e)
+    for t in ("fp64", "mixed"):
+        assert res[t, "learned"]["iterations"] <= 1.25 * res[t, "diagonal"]["iterations"]
+    h.set_preconditioner(None)
     h.close()
 
 
