@@ -210,7 +210,9 @@ int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma) {
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
   const size_t M = (size_t)na * nb;
   const bool tc = sizeof(T) == 4 && ab.tc_ready;
-  const size_t need = tc ? ab_tc_work_bytes(h) : sizeof(T) * M * (size_t)(ab.npq + ab.nrs);
+  const bool fused = tc && ab.tc_fused_stages > 0;
+  const size_t need = fused ? ab_tc_fused_work_bytes(h)
+                            : tc ? ab_tc_work_bytes(h) : sizeof(T) * M * (size_t)(ab.npq + ab.nrs);
   if (h->ab_work_bytes < need) {
     if (h->d_ab_work) cudaFree(h->d_ab_work);
     h->d_ab_work = nullptr;
@@ -220,7 +222,10 @@ int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma) {
   }
   const int grid = h->num_sms * 8;
   T *E = nullptr;
-  if (tc) {
+  if (fused) {
+    E = reinterpret_cast<T *>(h->d_ab_work);
+    TPB_CHECK(ab_tc_fused(h, reinterpret_cast<const float *>(C), reinterpret_cast<float *>(E), M));
+  } else if (tc) {
     const size_t Mp = (M + 127) / 128 * 128;
     E = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(h->d_ab_work) +
                               Mp * ab.Kp * 2 * sizeof(uint16_t));

@@ -148,6 +148,187 @@ __global__ void __launch_bounds__(128, 1)
   }
 }
 
+// Fused gather -> contraction: the A tiles are built in shared memory straight from C instead of
+// being gathered to HBM first.  Warp roles of a persistent CTA (288 threads, one per SM):
+//   warps 0-3  producers: thread r builds row r of the 128-row tile of determinants j = (Ja, Ib)
+//              in stage s -- zeroes it, then writes the split-BF16 s_b C[Ja, Jb] of every beta
+//              single Ib -> Jb (label rs) at column rs -- then fences the writes for the tensor
+//              core's proxy and arrives on full[s];
+//   warp 8     the MMA issuer: waits for full[s] and a free accumulator, issues 3 x Kp/16
+//              tcgen05.mma into it, commits to empty[s] (stage reusable) and acc_full[a];
+//   warps 4-7  the epilogue: wait acc_full[a], read their 32 TMEM lanes with tcgen05.ld, store E
+//              label-major, arrive on acc_empty[a].
+// NA A stages (2 when they fit beside the resident V operand, else 1) and two TMEM accumulators,
+// so the gather of tile t+1, the MMAs of tile t and the write-out of tile t-1 overlap.  The MMA
+// sequence and the hi/lo split are those of the unfused path, so E is the same.  Every wait is
+// bounded; an expired one records a code, stops the CTA's loops, and the MMA warp drains its
+// tensor-core work before TMEM is released.
+constexpr int kFusedThreads = 288;
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    ab_tc_fused_kernel(const float *__restrict__ C, uint32_t nb, const uint32_t *__restrict__ b_off,
+                       const uint32_t *__restrict__ b_ket, const int32_t *__restrict__ b_label,
+                       const __nv_bfloat16 *__restrict__ Bhi, const __nv_bfloat16 *__restrict__ Blo,
+                       float *__restrict__ E, int Kp, int Np, int npq, size_t M, size_t ntiles, int NA,
+                       int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const uint32_t b_bytes = (uint32_t)Np * Kp * 2, a_bytes = 128u * Kp * 2;
+  unsigned char *sBhi = smem, *sBlo = smem + b_bytes, *sA = smem + 2 * b_bytes;  // stage s: hi, lo
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sA + (size_t)NA * 2 * a_bytes);
+  // bars: [0,2) full, [2,4) empty, [4,6) acc_full, [6,8) acc_empty, 8 B loaded, 9 drain
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 10);
+  volatile int *status = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t ncols = 32;
+  while ((int)ncols < Np) ncols <<= 1;
+  auto bar = [&](int i) { return smem_addr(&bars[i]); };
+  auto fail_with = [&](int code) {
+    atomicExch(err, code);
+    *status = 1;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; s++) {
+      mbar_init(bar(s), 128);
+      mbar_init(bar(2 + s), 1);
+      mbar_init(bar(4 + s), 1);
+      mbar_init(bar(6 + s), 128);
+    }
+    mbar_init(bar(8), 1);
+    mbar_init(bar(9), 1);
+    fence_mbar_init();
+    *status = 0;
+  }
+  if (warp == 8) tmem_alloc(smem_addr(tmem_slot), 2 * ncols);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < 4) {
+    // ---------------- producers: build A tiles from C ----------------
+    const int r = threadIdx.x;
+    uint32_t it = 0;
+    for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+      if (*status) break;
+      const int s = (int)(it % (uint32_t)NA);
+      const uint32_t ph = (it / (uint32_t)NA) & 1u;
+      if (!mbar_wait(bar(2 + s), ph ^ 1u)) {
+        fail_with(11);
+        break;
+      }
+      unsigned char *hi = sA + (size_t)s * 2 * a_bytes, *lo = hi + a_bytes;
+      // row r of the canonical K-major layout: 16 bytes in each k-group's core matrix r/8
+      for (int g = 0; g < Kp / 8; g++) {
+        const uint32_t o = (uint32_t)((g * 16 + (r >> 3)) << 7) + ((r & 7) << 4);
+        *reinterpret_cast<uint4 *>(hi + o) = make_uint4(0, 0, 0, 0);
+        *reinterpret_cast<uint4 *>(lo + o) = make_uint4(0, 0, 0, 0);
+      }
+      const size_t j = tile * 128 + r;
+      if (j < M) {
+        const uint32_t ja = (uint32_t)(j / nb), ib = (uint32_t)(j - (size_t)ja * nb);
+        const float *crow = C + (size_t)ja * nb;
+        const uint32_t e1 = __ldg(&b_off[ib + 1]);
+        for (uint32_t e = __ldg(&b_off[ib]); e < e1; e++) {
+          const int32_t lab = __ldg(&b_label[e]);
+          float x = __ldg(&crow[__ldg(&b_ket[e])]);
+          if (lab < 0) x = -x;
+          const __nv_bfloat16 xh = __float2bfloat16_rn(x);
+          const __nv_bfloat16 xl = __float2bfloat16_rn(x - __bfloat162float(xh));
+          const int k = (lab > 0 ? lab : -lab) - 1;
+          const uint32_t o = (uint32_t)((((k >> 3) * 16 + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+          *reinterpret_cast<__nv_bfloat16 *>(hi + o) = xh;
+          *reinterpret_cast<__nv_bfloat16 *>(lo + o) = xl;
+        }
+      }
+      fence_proxy_async();
+      mbar_arrive(bar(s));
+    }
+  } else if (warp < 8) {
+    // ---------------- epilogue: TMEM -> E (label-major) ----------------
+    const int q = threadIdx.x - 128, ew = q >> 5;
+    uint32_t tc = 0;
+    for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tc++) {
+      if (*status) break;
+      const int a = (int)(tc & 1u);
+      const uint32_t aph = (tc >> 1) & 1u;
+      if (!mbar_wait(bar(4 + a), aph)) {
+        fail_with(12);
+        break;
+      }
+      fence_after_sync();
+      const size_t j = tile * 128 + q;
+      const uint32_t trow = tmem + (uint32_t)(a * (int)ncols) + ((uint32_t)(ew * 32) << 16);
+      for (int col = 0; col < Np; col += 16) {
+        float v[16];
+        tmem_ld16(trow + (uint32_t)col, v);
+        if (j < M) {
+#pragma unroll
+          for (int i = 0; i < 16; i++)
+            if (col + i < npq) E[(size_t)(col + i) * M + j] = v[i];
+        }
+      }
+      fence_before_sync();
+      mbar_arrive(bar(6 + a));
+    }
+  } else if (lane == 0) {
+    // ---------------- MMA issuer ----------------
+    mbar_expect_tx(bar(8), 2 * b_bytes);
+    bulk_g2s(smem_addr(sBhi), Bhi, b_bytes, bar(8));
+    bulk_g2s(smem_addr(sBlo), Blo, b_bytes, bar(8));
+    bool ok = mbar_wait(bar(8), 0);
+    if (!ok) {
+      fail_with(13);
+      mbar_wait(bar(8), 0);  // bounded second wait for the copies in flight
+    }
+    const int NG = Np >> 3;
+    const uint32_t b0 = smem_addr(sBhi), b1 = smem_addr(sBlo);
+    uint32_t it = 0;
+    for (size_t tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, it++) {
+      if (*status) break;
+      const int a = (int)(it & 1u);
+      const uint32_t aph = (it >> 1) & 1u;
+      const int s = (int)(it % (uint32_t)NA);
+      const uint32_t ph = (it / (uint32_t)NA) & 1u;
+      if (!mbar_wait(bar(6 + a), aph ^ 1u)) {
+        fail_with(14);
+        break;
+      }
+      if (!mbar_wait(bar(s), ph)) {
+        fail_with(15);
+        break;
+      }
+      fence_after_sync();
+      const uint32_t a0 = smem_addr(sA + (size_t)s * 2 * a_bytes), a1 = a0 + a_bytes;
+      for (int c = 0; c * 256 < Np; c++) {
+        const int nc = min(256, Np - c * 256);
+        const uint32_t idesc = idesc_bf16(nc);
+        const uint32_t td = tmem + (uint32_t)(a * (int)ncols) + (uint32_t)(c * 256);
+        for (int k16 = 0; k16 < Kp / 16; k16++) {
+          const uint32_t aoff = (uint32_t)(2 * k16) * 2048u;
+          const uint32_t boff = (uint32_t)((2 * k16) * NG + 32 * c) * 128u;
+          const uint64_t dah = make_desc(a0 + aoff, 2048u, 128u);
+          const uint64_t dal = make_desc(a1 + aoff, 2048u, 128u);
+          const uint64_t dbh = make_desc(b0 + boff, (uint32_t)NG * 128u, 128u);
+          const uint64_t dbl = make_desc(b1 + boff, (uint32_t)NG * 128u, 128u);
+          mma_bf16(td, dah, dbh, idesc, k16 > 0 ? 1u : 0u);
+          mma_bf16(td, dah, dbl, idesc, 1u);
+          mma_bf16(td, dal, dbh, idesc, 1u);
+        }
+      }
+      mma_commit(bar(2 + s));
+      mma_commit(bar(4 + a));
+    }
+    // drain: every tensor-core operation this thread issued has completed before TMEM goes
+    mma_commit(bar(9));
+    if (!mbar_wait(bar(9), 0)) fail_with(16);
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == 8) tmem_dealloc(tmem, 2 * ncols);
+}
+
 __global__ void ab_tc_gather_kernel(const float *__restrict__ C, uint32_t na, uint32_t nb,
                                     const uint32_t *__restrict__ b_off, const uint32_t *__restrict__ b_ket,
                                     const int32_t *__restrict__ b_label, int Kp,
@@ -168,6 +349,10 @@ __global__ void ab_tc_gather_kernel(const float *__restrict__ C, uint32_t na, ui
       Dlo[o] = lo;
     }
   }
+}
+
+size_t fused_smem(int Kp, int Np, int na) {
+  return (size_t)2 * Np * Kp * 2 + (size_t)na * 2 * 128 * Kp * 2 + 10 * 8 + 16;
 }
 
 }  // namespace
@@ -197,6 +382,18 @@ int ab_tc_setup(sbd_tpb_handle *h) {
   if (!ab.err) TPB_CUDA(cudaMalloc(&ab.err, sizeof(int)));
   TPB_CUDA(cudaMemset(ab.err, 0, sizeof(int)));
   TPB_CUDA(cudaFuncSetAttribute(ab_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // fused gather + contraction: two accumulators of up to 256 columns, V resident, one or two A stages
+  ab.tc_fused_stages = 0;
+  if (Np <= 256) {
+    for (int na = 2; na >= 1; na--) {
+      const size_t fs = fused_smem(Kp, Np, na);
+      if (fs <= h->smem_optin) {
+        TPB_CUDA(cudaFuncSetAttribute(ab_tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs));
+        ab.tc_fused_stages = na;
+        break;
+      }
+    }
+  }
   ab.tc_ready = true;
   return SBD_TPB_OK;
 }
@@ -205,6 +402,21 @@ size_t ab_tc_work_bytes(sbd_tpb_handle *h) {
   const ABDense &ab = h->ab;
   const size_t M = h->ndet(), Mp = (M + 127) / 128 * 128;
   return Mp * ab.Kp * 2 * sizeof(uint16_t) + M * (size_t)ab.npq * sizeof(float);
+}
+
+size_t ab_tc_fused_work_bytes(sbd_tpb_handle *h) { return h->ndet() * (size_t)h->ab.npq * sizeof(float); }
+
+int ab_tc_fused(sbd_tpb_handle *h, const float *C, float *E, size_t M) {
+  ABDense &ab = h->ab;
+  const size_t ntiles = (M + 127) / 128;
+  const size_t smem = fused_smem(ab.Kp, ab.Np, ab.tc_fused_stages);
+  const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)h->num_sms);
+  ab_tc_fused_kernel<<<grid, kFusedThreads, smem, h->stream>>>(
+      C, (uint32_t)h->bstr.size(), h->tb_s.off, h->tb_s.ket, ab.b_label,
+      reinterpret_cast<const __nv_bfloat16 *>(ab.Vhi), reinterpret_cast<const __nv_bfloat16 *>(ab.Vlo), E, ab.Kp,
+      ab.Np, ab.npq, M, ntiles, ab.tc_fused_stages, ab.err);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
 }
 
 int ab_tc_gather(sbd_tpb_handle *h, const float *C, size_t M) {

@@ -117,6 +117,7 @@ struct ABDense {
   // tensor-core path (FP32 sigma): V as BF16 hi/lo in the tcgen05 canonical layout
   bool tc_ready = false;
   int Kp = 0, Np = 0;
+  int tc_fused_stages = 0;        // A stages of the fused gather + contraction kernel (0: unfused)
   uint16_t *Vhi = nullptr, *Vlo = nullptr;
   int *err = nullptr;             // bounded-wait status of the tensor-core kernel
 };
