@@ -44,7 +44,8 @@ __global__ void ab_gather_kernel(const T *__restrict__ C, uint32_t na, uint32_t 
 template <typename T>
 __global__ void ab_scatter_kernel(const T *__restrict__ E, uint32_t na, uint32_t nb,
                                   const uint32_t *__restrict__ a_off, const uint32_t *__restrict__ a_ket,
-                                  const int32_t *__restrict__ a_label, size_t M, T *__restrict__ sigma) {
+                                  const int32_t *__restrict__ a_label, size_t M, T *__restrict__ sigma,
+                                  T scale) {
   const size_t total = (size_t)na * nb;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -55,7 +56,7 @@ __global__ void ab_scatter_kernel(const T *__restrict__ E, uint32_t na, uint32_t
       const T x = E[(size_t)((lab > 0 ? lab : -lab) - 1) * M + (size_t)a_ket[e] * nb + ib];
       acc += lab > 0 ? x : -x;
     }
-    sigma[i] += acc;
+    sigma[i] += acc * scale;
   }
 }
 
@@ -205,7 +206,7 @@ bool ab_dense_worthwhile(sbd_tpb_handle *h) {
 }
 
 template <typename T>
-int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma) {
+int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma, double scale) {
   ABDense &ab = h->ab;
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
   const size_t M = (size_t)na * nb;
@@ -242,13 +243,14 @@ int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma) {
     ab_gemm_kernel<T><<<g, 256, 0, h->stream>>>(V, D, E, ab.npq, ab.nrs, M);
     TPB_LAUNCHED(h);
   }
-  ab_scatter_kernel<T><<<grid, 256, 0, h->stream>>>(E, na, nb, h->ta_s.off, h->ta_s.ket, ab.a_label, M, sigma);
+  ab_scatter_kernel<T><<<grid, 256, 0, h->stream>>>(E, na, nb, h->ta_s.off, h->ta_s.ket, ab.a_label, M, sigma,
+                                                    (T)scale);
   TPB_LAUNCHED(h);
   if (tc) TPB_CHECK(ab_tc_check(h));
   return SBD_TPB_OK;
 }
 
-template int ab_dense_apply<double>(sbd_tpb_handle *, const double *, double *);
-template int ab_dense_apply<float>(sbd_tpb_handle *, const float *, float *);
+template int ab_dense_apply<double>(sbd_tpb_handle *, const double *, double *, double);
+template int ab_dense_apply<float>(sbd_tpb_handle *, const float *, float *, double);
 
 }  // namespace sbdtpb

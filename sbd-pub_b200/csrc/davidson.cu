@@ -126,18 +126,22 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
     cycle_steps = 0;
     for (int ib = 0; ib < nb; ib++) {
       const auto s0 = std::chrono::steady_clock::now();
-      // S_ib is exactly exchange-symmetric under the projection (every correction is projected,
-      // every other operation is elementwise), so its sigma takes the one-pass symmetric form
-      if (sym) TPB_CHECK(sigma_sep_sym<T>(h, S[ib].p, HS[ib].p, shift));
-      else TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
-      nsigma++;
       std::vector<const T *> cp(ib + 1);
       for (int k = 0; k <= ib; k++) cp[k] = S[k].p;
-      // the new column of the projected matrix and its Rayleigh-Ritz solve stay on the device;
-      // the residual kernel reads the Ritz coefficients from there
+      // S_ib is exactly exchange-symmetric under the projection (every correction is projected,
+      // every other operation is elementwise), so its sigma takes the one-pass symmetric form,
+      // whose transpose-add also forms the new column S_k . sigma(S_ib) of the projected matrix
+      if (sym) {
+        TPB_CHECK(sigma_sep_sym<T>(h, S[ib].p, HS[ib].p, shift, cp.data(), ib + 1, kOvSlot));
+      } else {
+        TPB_CHECK(sigma_sep_shift<T>(h, S[ib].p, HS[ib].p, 0, shift));
+        TPB_CHECK(multi_dot_async<T>(h, cp.data(), ib + 1, HS[ib].p, n, kOvSlot));
+      }
+      nsigma++;
+      // the Rayleigh-Ritz solve stays on the device; the residual kernel reads the Ritz
+      // coefficients from there
       ScaleArray fa;
       for (int k = 0; k < kMaxSub; k++) fa.v[k] = k <= ib ? f[k] : 0.0;
-      TPB_CHECK(multi_dot_async<T>(h, cp.data(), ib + 1, HS[ib].p, n, kOvSlot));
       TPB_CHECK(rr_solve(h, ib, fa, kOvSlot, kEigSlot));
       for (int k = 0; k < kMaxVec; k++) {
         ra.C.p[k] = k <= ib ? S[k].p : nullptr;
@@ -162,21 +166,32 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       // synchronisation.  If this step turns out converged, the extra work on t is discarded.
       const bool fast = !rec && !last && !(learned && cycle_mode == 1);
       double t0_fast = 0.0, tt_fast = 0.0;
-      TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
       std::vector<double> coef(ib + 1);
       for (int k = 0; k <= ib; k++) coef[k] = f[k] * f[k];
-      if (fast) {
-        if (sym) TPB_CHECK(symmetrize_async<T>(h, tnext, kSymSlot));
-        const int t0_slot = sym ? kSymSlot : 2 + ib + 1;
-        TPB_CHECK(cgs_update_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, n, 1, kCgsSlot));
-        TPB_CHECK(cgs_second_round_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, n, t0_slot,
-                                            kCgsSlot, kCgs2Slot));
+      if (fast && sym) {
+        // exchange-symmetric subspace: residual with the projection of t folded in and both
+        // Gram-Schmidt rounds in tile-pair form (half the subspace bytes of the general passes)
+        TPB_CHECK(residual_sym_async<T>(h, ra, 0));
+        TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, 1, kCgsSlot));
+        TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, 0, kCgs2Slot,
+                                   2 + ib + 1, kCgsSlot));
+      } else {
+        TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
+        if (fast) {
+          if (sym) TPB_CHECK(symmetrize_async<T>(h, tnext, kSymSlot));
+          const int t0_slot = sym ? kSymSlot : 2 + ib + 1;
+          TPB_CHECK(cgs_update_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, n, 1, kCgsSlot));
+          TPB_CHECK(cgs_second_round_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, n, t0_slot,
+                                              kCgsSlot, kCgs2Slot));
+        }
       }
       const double *sc = fetch_scalars(h, kScalarSlots);
       if (!sc) return SBD_TPB_ERR_CUDA;
       for (int k = 0; k < ib + 4; k++) out[k] = sc[k];  // W.W, r.r, S_k.t, t.t
       if (fast) {
-        t0_fast = sym ? sc[kSymSlot] : sc[2 + ib + 1];
+        // t.t after the projection: from the symmetrize pass, or (tile-pair residual, or no
+        // projection) from the residual pass itself
+        t0_fast = sym && !(fast && sym) ? sc[kSymSlot] : sc[2 + ib + 1];
         const double tt1 = sc[kCgsSlot];
         tt_fast = tt1 < 0.5 * t0_fast ? sc[kCgs2Slot] : tt1;
       }

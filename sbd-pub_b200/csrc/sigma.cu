@@ -385,6 +385,7 @@ struct AbSparseArgs {
   int L2;
   uint32_t nb;     // row length of C and sigma
   uint32_t group;  // singles staged per round
+  double scale;    // weight of the term (1; 1/2 before the symmetric sigma's transpose-add)
 };
 
 template <typename T, bool kStage>
@@ -445,13 +446,13 @@ __global__ void __launch_bounds__(256)
       uint32_t ib0, ib1;
       const double s0 = column(q, ib0), s1 = column(q + blockDim.x, ib1);
       const T o0 = srow[ib0], o1 = srow[ib1];
-      srow[ib0] = (T)((double)o0 + s0);
-      srow[ib1] = (T)((double)o1 + s1);
+      srow[ib0] = (T)((double)o0 + a.scale * s0);
+      srow[ib1] = (T)((double)o1 + a.scale * s1);
     }
     if (q < a.ncols_s) {
       uint32_t ib0;
       const double s0 = column(q, ib0);
-      srow[ib0] = (T)((double)srow[ib0] + s0);
+      srow[ib0] = (T)((double)srow[ib0] + a.scale * s0);
     }
   }
 }
@@ -533,11 +534,13 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   }
 }
 
-// The symmetric alpha pass: no C^T and no values kept for it, so one CTA per SM more than the
-// alpha pass of the general sigma fits without spills (FP32 8 and FP64 9 spill).
+// The symmetric alpha pass: no C^T and no values kept for it.  Launch shapes from a sweep (CUDA
+// events, ms at 4e8 / 1e8 determinants): FP32 2 row groups at 8 CTAs/SM 2.78 / 1.23 (a 148-byte
+// spill; 2/7 2.96 / 1.29, 4/8 3.02 / 1.30, 1/6 3.11 / 1.33, 2/6 3.32 / 1.40), FP64 2/8 4.83 / 2.08
+// (2/9 with a 192-byte spill 4.61 / 2.19, 2/7 5.18 / 2.18, 4/8 5.49 / 2.31, 1/4 6.43 / 2.68).
 template <typename T>
 int launch_block_sym(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out) {
-  if constexpr (sizeof(T) == 4) return launch_block_cfg<T, true, 2, 7, false, true>(h, ba, X, out, nullptr);
+  if constexpr (sizeof(T) == 4) return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
   else return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
 }
 
@@ -647,9 +650,10 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
 }
 
 template <typename T>
-int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma) {
+int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma, double scale = 1.0) {
   if (h->ab_nrows == 0 || h->ab_ncols == 0) return SBD_TPB_OK;
   AbSparseArgs a{};
+  a.scale = scale;
   a.rows = h->d_ab_rows;
   a.colp = h->d_ab_colp;
   a.bsp = h->d_ab_bsp;
@@ -766,13 +770,17 @@ int sigma_sep_shift(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, dou
 }
 
 // sigma = (H - shift) C for an exchange-symmetric C (C = C^T, alpha strings = beta strings): the
-// symmetric alpha pass writes B = (H_ii - shift) C / 2 + sum_Ja H_a(Ia, Ja) C[Ja, Ib], sym_add
-// forms B + B^T in place (the beta part of sigma is the transpose of the alpha part, and the
-// diagonal halves add back), then the alpha-beta term adds in as in sigma_sep_shift.  One
-// gathering pass instead of two and no C^T.  The result is exact up to rounding only when C is
-// symmetric; the caller guarantees that (Davidson with the exchange-symmetry projection).
+// symmetric alpha pass writes B = (H_ii - shift) C / 2 + sum_Ja H_a(Ia, Ja) C[Ja, Ib], the
+// alpha-beta term adds in at half weight (it is symmetric for a symmetric C), and sym_add forms
+// sigma = B + B^T in place: the beta part of sigma is the transpose of the alpha part, the halves
+// of the diagonal and alpha-beta terms add back.  One gathering pass instead of two and no C^T;
+// sigma comes out exactly symmetric.  The result is sigma up to rounding only when C is
+// symmetric; the caller guarantees that (Davidson with the exchange-symmetry projection).  With
+// m > 0 the transpose-add also reduces S_k . sigma for the m vectors S (exactly symmetric too)
+// into scalar slots slot.. (the Davidson step's new column of the projected matrix).
 template <typename T>
-int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift) {
+int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift, const T *const *S, int m,
+                  int slot) {
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
   if (na != nb || h->astr != h->bstr)
     return fail(SBD_TPB_ERR_STATE, "symmetric sigma needs identical alpha and beta strings");
@@ -806,21 +814,24 @@ int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift) {
   TPB_CUDA(cudaEventRecord(h->ev0, h->stream));
   TPB_CHECK(launch_block_sym<T>(h, ba, C, sigma));
   TPB_CUDA(cudaEventRecord(h->ev_k[0], h->stream));
-  TPB_CHECK(sym_add<T>(h, sigma));
-  TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
   if (dense_ab) {
-    TPB_CHECK(ab_dense_apply<T>(h, C, sigma));
+    TPB_CHECK(ab_dense_apply<T>(h, C, sigma, 0.5));
   } else {
-    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma));
+    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma, 0.5));
   }
+  TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
+  if (m > 0) TPB_CHECK(sym_add_dots<T>(h, sigma, S, m, slot));
+  else TPB_CHECK(sym_add<T>(h, sigma));
   TPB_CUDA(cudaEventRecord(h->ev_k[2], h->stream));
   h->sigma_kernels = 3;
   TPB_CUDA(cudaEventRecord(h->ev1, h->stream));
   return SBD_TPB_OK;
 }
 
-template int sigma_sep_sym<double>(sbd_tpb_handle *, const double *, double *, double);
-template int sigma_sep_sym<float>(sbd_tpb_handle *, const float *, float *, double);
+template int sigma_sep_sym<double>(sbd_tpb_handle *, const double *, double *, double, const double *const *,
+                                   int, int);
+template int sigma_sep_sym<float>(sbd_tpb_handle *, const float *, float *, double, const float *const *, int,
+                                  int);
 
 // Same two passes with a caller-provided C^T buffer and the alpha-beta terms always evaluated by
 // the direct loop of the alpha pass: needs no device memory beyond C, sigma and CT.

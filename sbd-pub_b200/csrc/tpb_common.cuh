@@ -227,7 +227,8 @@ int sigma_sep_given_ct(sbd_tpb_handle *h, const T *C, T *sigma, int accumulate, 
 // sigma = (H - shift) C for C = C^T over identical alpha and beta strings: one gathering pass and
 // an in-place B + B^T (see sigma.cu)
 template <typename T>
-int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift);
+int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift, const T *const *S = nullptr, int m = 0,
+                  int slot = 0);
 // per-block table sizes of the sigma launches, read back once per table build (blk_max, blk_for)
 int prepare_block_sizes(sbd_tpb_handle *h);
 int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y);
@@ -236,7 +237,7 @@ int reorder_sign_apply_f32(sbd_tpb_handle *h, const float *x, float *y);
 int ab_dense_setup(sbd_tpb_handle *h, int enable);
 bool ab_dense_worthwhile(sbd_tpb_handle *h);
 template <typename T>
-int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma);
+int ab_dense_apply(sbd_tpb_handle *h, const T *C, T *sigma, double scale = 1.0);
 // vecops.cu
 int ensure_partials(sbd_tpb_handle *h, size_t n);
 template <typename T>

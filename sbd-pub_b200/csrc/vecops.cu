@@ -351,6 +351,260 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint
   }
 }
 
+// t <- t + t^T in place (the symmetric sigma's B + B^T, tile pairs as symmetrize_kernel) and the
+// block partials of S_k . t_new for k < m: S_k and the new t are exactly symmetric, so the (bj, bi)
+// tile of a pair repeats the (bi, bj) tile's products and each off-diagonal pair is counted twice
+// from its (bi, bj) tile (half the S_k bytes of a separate dot pass, and no second read of t).
+template <typename T, int VW>
+__global__ void __launch_bounds__(256)
+    sym_add_dots_kernel(T *__restrict__ t, uint32_t nb, VecPtrs<T> S, int m, double *partials) {
+  constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;
+  __shared__ T A[TS][TS + 1], B[TS][TS + 1];
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, ty = threadIdx.x / TPR;
+  double acc[kMaxSub];
+#pragma unroll
+  for (int k = 0; k < kMaxSub; k++) acc[k] = 0.0;
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    uint32_t bi = (uint32_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
+    while (bi > 0 && (size_t)bi * nt - (size_t)bi * (bi - 1) / 2 > p) bi--;
+    while ((size_t)(bi + 1) * nt - (size_t)(bi + 1) * bi / 2 <= p) bi++;
+    const uint32_t bj = bi + (uint32_t)(p - ((size_t)bi * nt - (size_t)bi * (bi - 1) / 2));
+    __syncthreads();
+#pragma unroll
+    for (int r = ty; r < TS; r += RS) {
+      const uint32_t i = bi * TS + r, j = bj * TS + cx, i2 = bj * TS + r, j2 = bi * TS + cx;
+      T va[VW], vb[VW];
+      if (i < nb && j < nb) ldv<T, VW>(t + (size_t)i * nb + j, va);
+      else {
+#pragma unroll
+        for (int l = 0; l < VW; l++) va[l] = T(0);
+      }
+      if (i2 < nb && j2 < nb) ldv<T, VW>(t + (size_t)i2 * nb + j2, vb);
+      else {
+#pragma unroll
+        for (int l = 0; l < VW; l++) vb[l] = T(0);
+      }
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        A[r][cx + l] = va[l];
+        B[r][cx + l] = vb[l];
+      }
+    }
+    __syncthreads();
+    const double mult = bi == bj ? 1.0 : 2.0;
+#pragma unroll
+    for (int r = ty; r < TS; r += RS) {
+      const uint32_t i = bi * TS + r, j = bj * TS + cx;
+      T v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) v[l] = (T)((double)A[r][cx + l] + (double)B[cx + l][r]);
+      if (i < nb && j < nb) {
+        stv<T, VW>(t + (size_t)i * nb + j, v);
+#pragma unroll
+        for (int k = 0; k < kMaxSub; k++) {
+          if (k < m) {
+            T sv[VW];
+            ldv<T, VW>(S.p[k] + (size_t)i * nb + j, sv);
+            double d = 0.0;
+#pragma unroll
+            for (int l = 0; l < VW; l++) d += (double)v[l] * (double)sv[l];
+            acc[k] += mult * d;
+          }
+        }
+      }
+    }
+    if (bi != bj) {
+#pragma unroll
+      for (int r = ty; r < TS; r += RS) {
+        const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
+        T v[VW];
+#pragma unroll
+        for (int l = 0; l < VW; l++) v[l] = (T)((double)A[cx + l][r] + (double)B[r][cx + l]);
+        if (i2 < nb && j2 < nb) stv<T, VW>(t + (size_t)i2 * nb + j2, v);
+      }
+    }
+  }
+  block_reduce_store<kMaxSub>(acc, m, partials, gridDim.x);
+}
+
+// Tile-pair forms of the Davidson step's vector passes for exchange-symmetric subspaces (every S_k
+// and sigma(S_k) exactly symmetric: the symmetric sigma and the projection make them so).  Each
+// block walks 32 x 32 tile pairs (bi <= bj) as symmetrize_kernel does, reads the operands of the
+// (bi, bj) tile only, and writes the result to both tiles through shared memory; the reductions
+// count an off-diagonal pair's products twice.
+
+// tile-pair index p -> (bi, bj), bi <= bj, row-major over the upper triangle of nt x nt tiles
+__device__ __forceinline__ void tile_pair(size_t p, uint32_t nt, uint32_t &bi, uint32_t &bj) {
+  bi = (uint32_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
+  while (bi > 0 && (size_t)bi * nt - (size_t)bi * (bi - 1) / 2 > p) bi--;
+  while ((size_t)(bi + 1) * nt - (size_t)(bi + 1) * bi / 2 <= p) bi++;
+  bj = bi + (uint32_t)(p - ((size_t)bi * nt - (size_t)bi * (bi - 1) / 2));
+}
+
+// The residual pass with the exchange projection folded in: r = E' W - sum_k u_k sigma(S_k) on the
+// (bi, bj) tile (r is symmetric), t = r / (E0 - H_ii) at both (i, j) and (j, i) (H_ii differs
+// between the two in its last bits), t_sym = (t(i,j) + t(j,i)) / 2 written to both tiles -- what
+// residual_kernel followed by symmetrize_kernel produce, with half the subspace bytes read.
+// partials: [0] W.W, [1] r.r, [2+k] S_k.t_sym, [2+M] t_sym.t_sym.
+template <typename T, int VW, int M>
+__global__ void __launch_bounds__(256)
+    residual_sym_kernel(ResidualArgs<T> a, uint32_t nb, double *partials) {
+  constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;
+  __shared__ double Hd[TS][TS + 1];  // H_ii of the (bj, bi) tile
+  __shared__ T Tt[TS][TS + 1];       // t_sym of the (bi, bj) tile, read transposed for (bj, bi)
+  if (a.u_dev) {
+#pragma unroll
+    for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
+    a.e_shifted = __ldg(&a.e_dev[0]);
+    a.e0 = a.e_shifted + a.shift;
+  }
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, ty = threadIdx.x / TPR;
+  double acc[M + 3];
+#pragma unroll
+  for (int j = 0; j < M + 3; j++) acc[j] = 0.0;
+  auto hval = [&](size_t idx) -> double {
+    return a.hii32 ? a.e_shifted - (double)__ldg(&a.hii32[idx]) : a.e0 - __ldg(&a.hii[idx]);
+  };
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    uint32_t bi, bj;
+    tile_pair(p, nt, bi, bj);
+    __syncthreads();
+    // denominators E0 - H_ii of the (bj, bi) tile
+    for (int e = threadIdx.x; e < TS * TS; e += blockDim.x) {
+      const int rr = e / TS, cc = e % TS;
+      const uint32_t i2 = bj * TS + rr, j2 = bi * TS + cc;
+      Hd[rr][cc] = (i2 < nb && j2 < nb) ? hval((size_t)i2 * nb + j2) : 1.0;
+    }
+    __syncthreads();
+    const double mult = bi == bj ? 1.0 : 2.0;
+#pragma unroll
+    for (int r = ty; r < TS; r += RS) {
+      const uint32_t i = bi * TS + r, j = bj * TS + cx;
+      if (i >= nb || j >= nb) continue;
+      const size_t base = (size_t)i * nb + j;
+      T c[M][VW];
+      double w[VW], hc[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) w[l] = hc[l] = 0.0;
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        T hv[VW];
+        ldv<T, VW>(a.C.p[k] + base, c[k]);
+        ldv<T, VW>(a.HC.p[k] + base, hv);
+#pragma unroll
+        for (int l = 0; l < VW; l++) {
+          w[l] += a.u[k] * (double)c[k][l];
+          hc[l] += a.u[k] * (double)hv[l];
+        }
+      }
+      T v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        const double rv = a.e_shifted * w[l] - hc[l];
+        acc[0] += mult * w[l] * w[l];
+        acc[1] += mult * rv * rv;
+        const double d1 = hval(base + l), d2 = Hd[cx + l][r];
+        const T t1 = (T)((fabs(d1) > 1.0e-12) ? rv / d1 : rv / (d1 - 1.0e-12));
+        const T t2 = (T)((fabs(d2) > 1.0e-12) ? rv / d2 : rv / (d2 - 1.0e-12));
+        v[l] = (T)(((double)t1 + (double)t2) * 0.5);
+        Tt[r][cx + l] = v[l];
+#pragma unroll
+        for (int k = 0; k < M; k++) acc[2 + k] += mult * (double)c[k][l] * (double)v[l];
+        acc[2 + M] += mult * (double)v[l] * (double)v[l];
+      }
+      stv<T, VW>(a.t + base, v);
+    }
+    __syncthreads();
+    if (bi != bj) {
+#pragma unroll
+      for (int r = ty; r < TS; r += RS) {
+        const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
+        if (i2 >= nb || j2 >= nb) continue;
+        T v[VW];
+#pragma unroll
+        for (int l = 0; l < VW; l++) v[l] = Tt[cx + l][r];
+        stv<T, VW>(a.t + (size_t)i2 * nb + j2, v);
+      }
+    }
+  }
+  block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
+}
+
+// Gram-Schmidt round t -= sum_k o_k S_k on the (bi, bj) tile, written to both tiles; partials
+// [0] t.t, [1+k] S_k.t (kDots).  pred as in cgs_update_kernel.
+template <typename T, int VW, int M, bool kDots>
+__global__ void __launch_bounds__(256)
+    cgs_sym_kernel(VecPtrs<T> C, CoefArray co, const double *__restrict__ ov, T *__restrict__ t, uint32_t nb,
+                   double *partials, const double *__restrict__ pred0, const double *__restrict__ pred1) {
+  constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;
+  __shared__ T Tt[TS][TS + 1];
+  double acc[M + 1];
+#pragma unroll
+  for (int j = 0; j < M + 1; j++) acc[j] = 0.0;
+  if (pred0 && !(__ldg(pred1) < 0.5 * __ldg(pred0))) {
+    if (threadIdx.x <= (kDots ? M : 0)) partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = 0.0;
+    return;
+  }
+  double o[M];
+#pragma unroll
+  for (int k = 0; k < M; k++) o[k] = co.v[k] * (ov ? __ldg(&ov[k]) : 1.0);
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, ty = threadIdx.x / TPR;
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    uint32_t bi, bj;
+    tile_pair(p, nt, bi, bj);
+    const double mult = bi == bj ? 1.0 : 2.0;
+    __syncthreads();
+#pragma unroll
+    for (int r = ty; r < TS; r += RS) {
+      const uint32_t i = bi * TS + r, j = bj * TS + cx;
+      if (i >= nb || j >= nb) continue;
+      const size_t base = (size_t)i * nb + j;
+      T tv[VW], c[M][VW];
+      ldv<T, VW>(t + base, tv);
+      double x[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) x[l] = (double)tv[l];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        ldv<T, VW>(C.p[k] + base, c[k]);
+#pragma unroll
+        for (int l = 0; l < VW; l++) x[l] -= o[k] * (double)c[k][l];
+      }
+      T xt[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        xt[l] = (T)x[l];
+        Tt[r][cx + l] = xt[l];
+        acc[0] += mult * (double)xt[l] * (double)xt[l];
+        if (kDots) {
+#pragma unroll
+          for (int k = 0; k < M; k++) acc[1 + k] += mult * (double)c[k][l] * (double)xt[l];
+        }
+      }
+      stv<T, VW>(t + base, xt);
+    }
+    __syncthreads();
+    if (bi != bj) {
+#pragma unroll
+      for (int r = ty; r < TS; r += RS) {
+        const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
+        if (i2 >= nb || j2 >= nb) continue;
+        T v[VW];
+#pragma unroll
+        for (int l = 0; l < VW; l++) v[l] = Tt[cx + l][r];
+        stv<T, VW>(t + (size_t)i2 * nb + j2, v);
+      }
+    }
+  }
+  block_reduce_store<M + 1>(acc, kDots ? M + 1 : 1, partials, gridDim.x);
+}
+
 // Rayleigh-Ritz of the Davidson subspace on one warp.  Hs (ld kMaxSub, column-major, persistent
 // across the steps of a cycle) gets column and row ib = f_k f_ib ov_k; the leading n = ib + 1
 // block is diagonalised by cyclic Jacobi rotations in shared memory (each rotation's row and
@@ -689,6 +943,99 @@ int sym_add(sbd_tpb_handle *h, T *x) {
 }
 
 template <typename T>
+int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
+  if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = h->num_sms * kSymBlocksPerSm;
+  TPB_CHECK(ensure_partials(h, std::max<size_t>((size_t)(kMaxVec + 3) * vec_blocks(h) + kMaxVec + 3,
+                                                (size_t)kMaxSub * nblk + 1)));
+  VecPtrs<T> P;
+  for (int j = 0; j < kMaxVec; j++) P.p[j] = j < m ? S[j] : nullptr;
+  constexpr int VW = 16 / sizeof(T);
+  bool vec = nb % VW == 0 && reinterpret_cast<uintptr_t>(x) % 16 == 0;
+  for (int j = 0; j < m; j++) vec = vec && reinterpret_cast<uintptr_t>(S[j]) % 16 == 0;
+  if (vec) sym_add_dots_kernel<T, VW><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+  else sym_add_dots_kernel<T, 1><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+  TPB_LAUNCHED(h);
+  return reduce_into(h, m, h->d_scal + slot, nblk);
+}
+
+template <typename T>
+static bool pair_vec_ok(uint32_t nb, const void *const *ptrs, int count) {
+  constexpr int VW = 16 / sizeof(T);
+  if (nb % VW) return false;
+  for (int j = 0; j < count; j++)
+    if (ptrs[j] && reinterpret_cast<uintptr_t>(ptrs[j]) % 16) return false;
+  return true;
+}
+
+template <typename T>
+int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
+  if (a.m < 1 || a.m > kMaxSub || !a.t || a.W) return fail(SBD_TPB_ERR_INVALID, "residual_sym: bad arguments");
+  TPB_CHECK(ensure_scalars(h));
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = h->num_sms * kSymBlocksPerSm;
+  TPB_CHECK(ensure_partials(h, std::max<size_t>((size_t)(kMaxVec + 3) * vec_blocks(h) + kMaxVec + 3,
+                                                (size_t)(kMaxSub + 3) * nblk + 1)));
+  const void *ptrs[2 * kMaxSub + 1];
+  int np = 0;
+  for (int k = 0; k < a.m; k++) {
+    ptrs[np++] = a.C.p[k];
+    ptrs[np++] = a.HC.p[k];
+  }
+  ptrs[np++] = a.t;
+  const bool vec = pair_vec_ok<T>(nb, ptrs, np);
+  TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      if (vec) residual_sym_kernel<T, 16 / sizeof(T), M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, a.m + 3, h->d_scal + slot, nblk);
+}
+
+template <typename T>
+int cgs_sym_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                  int want_dots, int slot, int t0_slot, int tt_slot) {
+  if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
+  TPB_CHECK(ensure_scalars(h));
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = h->num_sms * kSymBlocksPerSm;
+  TPB_CHECK(ensure_partials(h, std::max<size_t>((size_t)(kMaxVec + 3) * vec_blocks(h) + kMaxVec + 3,
+                                                (size_t)(kMaxSub + 1) * nblk + 1)));
+  VecPtrs<T> P;
+  CoefArray co;
+  const void *ptrs[kMaxSub + 1];
+  for (int j = 0; j < kMaxVec; j++) P.p[j] = j < m ? C[j] : nullptr;
+  for (int j = 0; j < kMaxSub; j++) co.v[j] = j < m ? coef[j] : 0.0;
+  for (int j = 0; j < m; j++) ptrs[j] = C[j];
+  ptrs[m] = t;
+  const bool vec = pair_vec_ok<T>(nb, ptrs, m + 1);
+  const double *p0 = t0_slot >= 0 ? h->d_scal + t0_slot : nullptr;
+  const double *p1 = t0_slot >= 0 ? h->d_scal + tt_slot : nullptr;
+  TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      constexpr int VW = 16 / sizeof(T);
+      if (want_dots) {
+        if (vec) cgs_sym_kernel<T, VW, M, true><<<nblk, 256, 0, h->stream>>>(P, co, h->d_scal + ov_slot, t, nb, h->d_partials, p0, p1);
+        else cgs_sym_kernel<T, 1, M, true><<<nblk, 256, 0, h->stream>>>(P, co, h->d_scal + ov_slot, t, nb, h->d_partials, p0, p1);
+      } else {
+        if (vec) cgs_sym_kernel<T, VW, M, false><<<nblk, 256, 0, h->stream>>>(P, co, h->d_scal + ov_slot, t, nb, h->d_partials, p0, p1);
+        else cgs_sym_kernel<T, 1, M, false><<<nblk, 256, 0, h->stream>>>(P, co, h->d_scal + ov_slot, t, nb, h->d_partials, p0, p1);
+      }
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, want_dots ? 1 + m : 1, h->d_scal + slot, nblk);
+}
+
+template <typename T>
 int scale_vec(sbd_tpb_handle *h, T *x, double a, size_t n) {
   scale_kernel<T><<<vec_blocks(h), kVecThreads, 0, h->stream>>>(x, a, n);
   TPB_LAUNCHED(h);
@@ -715,6 +1062,14 @@ template int cgs_second_round_async<double>(sbd_tpb_handle *, const double *cons
                                             double *, size_t, int, int, int);
 template int cgs_second_round_async<float>(sbd_tpb_handle *, const float *const *, int, const double *, int,
                                            float *, size_t, int, int, int);
+template int sym_add_dots<double>(sbd_tpb_handle *, double *, const double *const *, int, int);
+template int sym_add_dots<float>(sbd_tpb_handle *, float *, const float *const *, int, int);
+template int residual_sym_async<double>(sbd_tpb_handle *, const ResidualArgs<double> &, int);
+template int residual_sym_async<float>(sbd_tpb_handle *, const ResidualArgs<float> &, int);
+template int cgs_sym_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, int, double *, int,
+                                   int, int, int);
+template int cgs_sym_async<float>(sbd_tpb_handle *, const float *const *, int, const double *, int, float *, int,
+                                  int, int, int);
 template int sym_add<double>(sbd_tpb_handle *, double *);
 template int sym_add<float>(sbd_tpb_handle *, float *);
 template int multi_dot<double>(sbd_tpb_handle *, const double *const *, int, const double *,

@@ -49,6 +49,19 @@ int symmetrize(sbd_tpb_handle *h, T *t, double *tt);
 // x <- x + x^T over the square determinant matrix (in place, no reduction)
 template <typename T>
 int sym_add(sbd_tpb_handle *h, T *x);
+// Exchange-symmetric subspace (every S_k and sigma(S_k) exactly symmetric): the residual pass with
+// the projection of t folded in, reading one tile of each 32 x 32 tile pair (no W; slots as
+// residual_step_async: W.W, r.r, S_k.t, t.t), and a Gram-Schmidt round the same way (slots: t.t,
+// S_k.t with want_dots; t0_slot >= 0 makes it the device-decided second round of
+// cgs_second_round_async).
+template <typename T>
+int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot);
+template <typename T>
+int cgs_sym_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
+                  int want_dots, int slot, int t0_slot = -1, int tt_slot = -1);
+// the same, and S_k . x_new (k < m, S_k exactly symmetric) into scalar slots slot..
+template <typename T>
+int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot);
 
 // The same passes without a host round trip: each reduces into slots of a small device array
 // (kScalarSlots doubles), read back together by fetch_scalars (one stream synchronisation).

@@ -120,3 +120,26 @@ def test_wide_subspace_and_restart_limits():
     assert r["energy"] == pytest.approx(e_or, abs=1e-8)
     r2 = h.davidson(sbd_tpb.default_params(max_it=400, max_nb=3, eps=1e-6), want_vector=False)
     assert r2["converged"] and r2["energy"] == pytest.approx(e_or, abs=1e-8)
+
+
+def test_release_work_memory():
+    """sbd_tpb_release_work gives back the Davidson vectors kept between solves and the sigma
+    staging; the next solve allocates them again and gives the same answer."""
+    import torch
+
+    import sbd_tpb
+    import synth
+    prob = synth.make_problem("sci24", nstrings=1500)
+    h = sbd_tpb.Handle(0)
+    h.set_problem(prob)
+    p = sbd_tpb.default_params(max_it=20, max_nb=8, eps=1e-6)
+    r1 = h.davidson(p, want_vector=False)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    h.free_vectors()
+    free_after, _ = torch.cuda.mem_get_info()
+    # at least the 17 FP64 N-vectors of an 8-vector subspace (S, sigma(S), W)
+    assert free_after - free_before >= 17 * prob.ndet * 8
+    r2 = h.davidson(p, want_vector=False)
+    assert r2["energy"] == r1["energy"] and r2["iterations"] == r1["iterations"]
+    h.close()
