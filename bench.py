@@ -105,6 +105,19 @@ ACCURACY = [
     ("sci28", 1e-6, 1e-4, 8, 8),
     ("sci36", 1e-6, 1e-4, 4, 6),
 ]
+# restart cycles allowed per solve: 1,200 steps at most, so the 4-vector FP64 run can converge
+ACCURACY_MAX_STEPS = 1200
+
+
+def spin_squared(two, L, n_beta):
+    """<S^2> of a vector with S_z = 0 from its opposite-spin 2-RDM block in the reference layout
+    (twobody[s + 2t][i + L j + L^2 k + L^3 l] = <c+_is c+_jt c_lt c_ks>, block s=alpha, t=beta):
+    <S^2> = S_z^2 + S_z + N_beta - sum_pq <a+_{p alpha} a+_{q beta} a_{p beta} a_{q alpha}>."""
+    L2 = L * L
+    blk = np.asarray(two)[2 * L2 * L2: 3 * L2 * L2]
+    p = np.arange(L)
+    P, Q = np.meshgrid(p, p, indexing="ij")
+    return float(n_beta - blk[P + L * Q + L2 * Q + L2 * L * P].sum())
 
 
 def accuracy_report(args, local):
@@ -128,20 +141,25 @@ def accuracy_report(args, local):
             if pre == sbd_tpb.PRECOND_LEARNED:
                 h.set_preconditioner(pc)
             t0 = time.perf_counter()
-            r = h.davidson(sbd_tpb.default_params(max_it=60, max_nb=nb_, eps=e_, precision=prec,
-                                                  preconditioner=pre), want_vector=False, want_rdm=True)
-            runs[tag] = dict(r, seconds_wall=time.perf_counter() - t0)
+            r = h.davidson(sbd_tpb.default_params(max_it=ACCURACY_MAX_STEPS // nb_, max_nb=nb_, eps=e_,
+                                                  precision=prec, preconditioner=pre),
+                           want_vector=False, want_rdm=True)
+            runs[tag] = dict(r, seconds_wall=time.perf_counter() - t0,
+                             spin_squared=spin_squared(r["two"], h.problem.norb,
+                                                       bin(int(h.problem.bstr[0])).count("1")))
             h.set_preconditioner(None)
             h.free_vectors()
         ref = runs["fp64"]
         rec = {"determinants": h.problem.ndet, "fp64": {"energy": ref["energy"], "residual": ref["residual"],
+                                                         "converged": ref["converged"],
                                                          "sigma_steps": ref["iterations"],
                                                          "seconds": ref["seconds_wall"], "eps": eps64,
-                                                         "subspace": nb64}}
+                                                         "subspace": nb64, "spin_squared": ref["spin_squared"]}}
         for tag in ("mixed", "mixed_learned"):
             r = runs[tag]
             rec[tag] = {"energy": r["energy"], "abs_energy_error": abs(r["energy"] - ref["energy"]),
-                        "fp64_residual": r["residual"], "sigma_steps": r["iterations"],
+                        "fp64_residual": r["residual"], "converged": r["converged"],
+                        "spin_squared": r["spin_squared"], "sigma_steps": r["iterations"],
                         "learned_steps": r["learned_steps"], "fallback_steps": r["fallback_steps"],
                         "seconds": r["seconds_wall"], "eps": eps, "subspace": nbm,
                         "max_abs_1rdm_error": float(np.max(np.abs(r["one"] - ref["one"]))),

@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         const uint32_t ja = (uint32_t)(j / nb), ib = (uint32_t)(j - (size_t)ja * nb);
         const float *crow = C + (size_t)ja * nb;
         const uint32_t e1 = __ldg(&b_off[ib + 1]);
+#pragma unroll 4
         for (uint32_t e = __ldg(&b_off[ib]); e < e1; e++) {
           const int32_t lab = __ldg(&b_label[e]);
           float x = __ldg(&crow[__ldg(&b_ket[e])]);
@@ -259,13 +260,22 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       fence_after_sync();
       const size_t j = tile * 128 + q;
       const uint32_t trow = tmem + (uint32_t)(a * (int)ncols) + ((uint32_t)(ew * 32) << 16);
+      // the next 16 columns load from TMEM while this 16 go out to E
+      uint32_t ra[16], rb[16];
+      tmem_ld16_issue(trow, ra);
+      tmem_ld_wait16(ra);
       for (int col = 0; col < Np; col += 16) {
-        float v[16];
-        tmem_ld16(trow + (uint32_t)col, v);
+        const bool more = col + 16 < Np;
+        if (more) tmem_ld16_issue(trow + (uint32_t)(col + 16), rb);
         if (j < M) {
 #pragma unroll
           for (int i = 0; i < 16; i++)
-            if (col + i < npq) E[(size_t)(col + i) * M + j] = v[i];
+            if (col + i < npq) E[(size_t)(col + i) * M + j] = __uint_as_float(ra[i]);
+        }
+        if (more) {
+          tmem_ld_wait16(rb);
+#pragma unroll
+          for (int i = 0; i < 16; i++) ra[i] = rb[i];
         }
       }
       fence_before_sync();
