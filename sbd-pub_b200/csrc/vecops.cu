@@ -452,8 +452,9 @@ template <typename T, int VW, int M>
 __global__ void __launch_bounds__(256)
     residual_sym_kernel(ResidualArgs<T> a, uint32_t nb, double *partials) {
   constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;
-  __shared__ double Hd[TS][TS + 1];  // H_ii of the (bj, bi) tile
-  __shared__ T Tt[TS][TS + 1];       // t_sym of the (bi, bj) tile, read transposed for (bj, bi)
+  // the diagonal of the (bj, bi) tile as stored: H_ii - H_00 in FP32 for FP32 vectors, H_ii in FP64
+  __shared__ T Hd[TS][TS + 1];
+  __shared__ T Tt[TS][TS + 1];  // t_sym of the (bi, bj) tile, read transposed for (bj, bi)
   if (a.u_dev) {
 #pragma unroll
     for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
@@ -466,18 +467,18 @@ __global__ void __launch_bounds__(256)
   double acc[M + 3];
 #pragma unroll
   for (int j = 0; j < M + 3; j++) acc[j] = 0.0;
-  auto hval = [&](size_t idx) -> double {
-    return a.hii32 ? a.e_shifted - (double)__ldg(&a.hii32[idx]) : a.e0 - __ldg(&a.hii[idx]);
-  };
+  // E0 - H_ii from the stored diagonal value (as residual_kernel forms it)
+  auto hdiff = [&](T hv) -> double { return sizeof(T) == 4 ? a.e_shifted - (double)hv : a.e0 - (double)hv; };
+  const T *hsrc = sizeof(T) == 4 ? reinterpret_cast<const T *>(a.hii32) : reinterpret_cast<const T *>(a.hii);
   for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
     uint32_t bi, bj;
     tile_pair(p, nt, bi, bj);
     __syncthreads();
-    // denominators E0 - H_ii of the (bj, bi) tile
+    // the diagonal of the (bj, bi) tile
     for (int e = threadIdx.x; e < TS * TS; e += blockDim.x) {
       const int rr = e / TS, cc = e % TS;
       const uint32_t i2 = bj * TS + rr, j2 = bi * TS + cc;
-      Hd[rr][cc] = (i2 < nb && j2 < nb) ? hval((size_t)i2 * nb + j2) : 1.0;
+      Hd[rr][cc] = (i2 < nb && j2 < nb) ? __ldg(&hsrc[(size_t)i2 * nb + j2]) : T(0);
     }
     __syncthreads();
     const double mult = bi == bj ? 1.0 : 2.0;
@@ -507,7 +508,7 @@ __global__ void __launch_bounds__(256)
         const double rv = a.e_shifted * w[l] - hc[l];
         acc[0] += mult * w[l] * w[l];
         acc[1] += mult * rv * rv;
-        const double d1 = hval(base + l), d2 = Hd[cx + l][r];
+        const double d1 = hdiff(__ldg(&hsrc[base + l])), d2 = hdiff(Hd[cx + l][r]);
         const T t1 = (T)((fabs(d1) > 1.0e-12) ? rv / d1 : rv / (d1 - 1.0e-12));
         const T t2 = (T)((fabs(d2) > 1.0e-12) ? rv / d2 : rv / (d2 - 1.0e-12));
         v[l] = (T)(((double)t1 + (double)t2) * 0.5);
@@ -603,6 +604,153 @@ __global__ void __launch_bounds__(256)
     }
   }
   block_reduce_store<M + 1>(acc, kDots ? M + 1 : 1, partials, gridDim.x);
+}
+
+// FP32 forms of the two tile-pair passes above for 16-byte rows (32 x 32 tiles, one tile row per
+// thread): every global load of a tile pair -- the thread's rows of both tiles, of the S_k / sigma(S_k)
+// it multiplies, and of the diagonal -- is issued before the first barrier, so a tile pair waits on one
+// round of memory latency instead of two or three (the general forms loaded the subspace tiles only
+// after the barrier and ran FP32 at ~3 TB/s).  Same arithmetic, same order per element.
+template <int M>
+__global__ void __launch_bounds__(256)
+    sym_add_dots_f32_kernel(float *__restrict__ t, uint32_t nb, VecPtrs<float> S, double *partials) {
+  constexpr int TS = kSymTile, VW = 4, TPR = TS / VW;
+  static_assert(256 / TPR == TS, "one tile row per thread");
+  __shared__ float A[TS][TS + 1], B[TS][TS + 1];
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, r = threadIdx.x / TPR;
+  double acc[M];
+#pragma unroll
+  for (int k = 0; k < M; k++) acc[k] = 0.0;
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    uint32_t bi, bj;
+    tile_pair(p, nt, bi, bj);
+    const uint32_t i = bi * TS + r, j = bj * TS + cx, i2 = bj * TS + r, j2 = bi * TS + cx;
+    const bool in1 = i < nb && j < nb, in2 = i2 < nb && j2 < nb;
+    float va[VW] = {0.f, 0.f, 0.f, 0.f}, vb[VW] = {0.f, 0.f, 0.f, 0.f}, sv[M][VW];
+    if (in1) ldv<float, VW>(t + (size_t)i * nb + j, va);
+    if (in2) ldv<float, VW>(t + (size_t)i2 * nb + j2, vb);
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+      if (in1) ldv<float, VW>(S.p[k] + (size_t)i * nb + j, sv[k]);
+      else {
+#pragma unroll
+        for (int l = 0; l < VW; l++) sv[k][l] = 0.f;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < VW; l++) {
+      A[r][cx + l] = va[l];
+      B[r][cx + l] = vb[l];
+    }
+    __syncthreads();
+    const double mult = bi == bj ? 1.0 : 2.0;
+    if (in1) {
+      float v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) v[l] = (float)((double)A[r][cx + l] + (double)B[cx + l][r]);
+      stv<float, VW>(t + (size_t)i * nb + j, v);
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        double d = 0.0;
+#pragma unroll
+        for (int l = 0; l < VW; l++) d += (double)v[l] * (double)sv[k][l];
+        acc[k] += mult * d;
+      }
+    }
+    if (bi != bj && in2) {
+      float v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) v[l] = (float)((double)A[cx + l][r] + (double)B[r][cx + l]);
+      stv<float, VW>(t + (size_t)i2 * nb + j2, v);
+    }
+  }
+  block_reduce_store<M>(acc, M, partials, gridDim.x);
+}
+
+template <int M>
+__global__ void __launch_bounds__(256)
+    residual_sym_f32_kernel(ResidualArgs<float> a, uint32_t nb, double *partials) {
+  constexpr int TS = kSymTile, VW = 4, TPR = TS / VW;
+  static_assert(256 / TPR == TS, "one tile row per thread");
+  __shared__ float Hd[TS][TS + 1];  // H_ii - H_00 of the (bj, bi) tile
+  __shared__ float Tt[TS][TS + 1];  // t_sym of the (bi, bj) tile, read transposed for (bj, bi)
+  if (a.u_dev) {
+#pragma unroll
+    for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
+    a.e_shifted = __ldg(&a.e_dev[0]);
+    a.e0 = a.e_shifted + a.shift;
+  }
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, r = threadIdx.x / TPR;
+  double acc[M + 3];
+#pragma unroll
+  for (int k = 0; k < M + 3; k++) acc[k] = 0.0;
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    uint32_t bi, bj;
+    tile_pair(p, nt, bi, bj);
+    const uint32_t i = bi * TS + r, j = bj * TS + cx, i2 = bj * TS + r, j2 = bi * TS + cx;
+    const bool in1 = i < nb && j < nb, in2 = i2 < nb && j2 < nb;
+    const size_t base = (size_t)i * nb + j;
+    float c[M][VW], hv[M][VW], hij[VW] = {0.f, 0.f, 0.f, 0.f}, hji[VW] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+      if (in1) {
+        ldv<float, VW>(a.C.p[k] + base, c[k]);
+        ldv<float, VW>(a.HC.p[k] + base, hv[k]);
+      } else {
+#pragma unroll
+        for (int l = 0; l < VW; l++) c[k][l] = hv[k][l] = 0.f;
+      }
+    }
+    if (in1) ldv<float, VW>(a.hii32 + base, hij);
+    if (in2) ldv<float, VW>(a.hii32 + (size_t)i2 * nb + j2, hji);
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < VW; l++) Hd[r][cx + l] = hji[l];
+    __syncthreads();
+    const double mult = bi == bj ? 1.0 : 2.0;
+    if (in1) {
+      double w[VW], hc[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) w[l] = hc[l] = 0.0;
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+#pragma unroll
+        for (int l = 0; l < VW; l++) {
+          w[l] += a.u[k] * (double)c[k][l];
+          hc[l] += a.u[k] * (double)hv[k][l];
+        }
+      }
+      float v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        const double rv = a.e_shifted * w[l] - hc[l];
+        acc[0] += mult * w[l] * w[l];
+        acc[1] += mult * rv * rv;
+        const double d1 = a.e_shifted - (double)hij[l], d2 = a.e_shifted - (double)Hd[cx + l][r];
+        const float t1 = (float)((fabs(d1) > 1.0e-12) ? rv / d1 : rv / (d1 - 1.0e-12));
+        const float t2 = (float)((fabs(d2) > 1.0e-12) ? rv / d2 : rv / (d2 - 1.0e-12));
+        v[l] = (float)(((double)t1 + (double)t2) * 0.5);
+        Tt[r][cx + l] = v[l];
+#pragma unroll
+        for (int k = 0; k < M; k++) acc[2 + k] += mult * (double)c[k][l] * (double)v[l];
+        acc[2 + M] += mult * (double)v[l] * (double)v[l];
+      }
+      stv<float, VW>(a.t + base, v);
+    }
+    __syncthreads();
+    if (bi != bj && in2) {
+      float v[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) v[l] = Tt[cx + l][r];
+      stv<float, VW>(a.t + (size_t)i2 * nb + j2, v);
+    }
+  }
+  block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
 }
 
 // Rayleigh-Ritz of the Davidson subspace on one warp.  Hs (ld kMaxSub, column-major, persistent
@@ -955,9 +1103,22 @@ int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
   constexpr int VW = 16 / sizeof(T);
   bool vec = nb % VW == 0 && reinterpret_cast<uintptr_t>(x) % 16 == 0;
   for (int j = 0; j < m; j++) vec = vec && reinterpret_cast<uintptr_t>(S[j]) % 16 == 0;
-  if (vec) sym_add_dots_kernel<T, VW><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
-  else sym_add_dots_kernel<T, 1><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
-  TPB_LAUNCHED(h);
+  if (vec && sizeof(T) == 4) {
+    TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
+      constexpr int M = decltype(K)::value;
+      if constexpr (M <= kMaxSub) {
+        sym_add_dots_f32_kernel<M><<<nblk, 256, 0, h->stream>>>(reinterpret_cast<float *>(x), nb,
+                                                                 *reinterpret_cast<VecPtrs<float> *>(&P),
+                                                                 h->d_partials);
+        TPB_LAUNCHED(h);
+      }
+      return SBD_TPB_OK;
+    }));
+  } else {
+    if (vec) sym_add_dots_kernel<T, VW><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+    else sym_add_dots_kernel<T, 1><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+    TPB_LAUNCHED(h);
+  }
   return reduce_into(h, m, h->d_scal + slot, nblk);
 }
 
@@ -972,7 +1133,8 @@ static bool pair_vec_ok(uint32_t nb, const void *const *ptrs, int count) {
 
 template <typename T>
 int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
-  if (a.m < 1 || a.m > kMaxSub || !a.t || a.W) return fail(SBD_TPB_ERR_INVALID, "residual_sym: bad arguments");
+  if (a.m < 1 || a.m > kMaxSub || !a.t || a.W || (sizeof(T) == 4) != (a.hii32 != nullptr))
+    return fail(SBD_TPB_ERR_INVALID, "residual_sym: bad arguments");
   TPB_CHECK(ensure_scalars(h));
   const uint32_t nb = (uint32_t)h->bstr.size();
   const int nblk = h->num_sms * kSymBlocksPerSm;
@@ -989,8 +1151,13 @@ int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
   TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
     constexpr int M = decltype(K)::value;
     if constexpr (M <= kMaxSub) {
-      if (vec) residual_sym_kernel<T, 16 / sizeof(T), M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
-      else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      if constexpr (sizeof(T) == 4) {
+        if (vec) residual_sym_f32_kernel<M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+        else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      } else {
+        if (vec) residual_sym_kernel<T, 16 / sizeof(T), M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+        else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      }
       TPB_LAUNCHED(h);
     }
     return SBD_TPB_OK;
