@@ -91,13 +91,21 @@ def test_sigma_fp32(tpb, oracle, name):
 
 
 def test_sigma_fci12_vs_reference_sample(tpb, oracle):
-    """FCI (853,776 determinants, dense alpha-beta path): sigma of the reference's converged
-    vector reproduces its energy, and the oracle's sigma on a row subset."""
+    """FCI (853,776 determinants): sigma of the converged vector reproduces the reference's energy, and
+    equals the oracle's sigma (orc_sigma_rows, the reference's per-element order) on 200 sampled
+    determinants, in FP64 and (dense alpha-beta path on the tensor cores) in FP32."""
     h, prob, g, meta = _handle(tpb, "fci12")
     r = h.davidson(tpb.default_params(max_it=10, max_nb=10, eps=1e-8))
     W = r["W"]
     sw = h.sigma(W)
     assert abs(float(W @ sw) - meta["energy"]) < 1e-8
+    ham = oracle.Hamiltonian.from_arrays(prob.norb, prob.nelec, prob.core, prob.h1, prob.eri_packed)
+    rows = np.random.default_rng(12).choice(prob.ndet, size=200, replace=False)
+    ref = oracle.System(ham, prob.astr, prob.bstr).sigma_rows(rows, W)
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(sw[rows] - ref)) <= 1e-12 * scale
+    s32 = h.sigma(W.astype(np.float32))
+    assert np.max(np.abs(s32[rows] - ref)) <= 2e-5 * scale
 
 
 @pytest.mark.parametrize("name", WITH_FCI)
