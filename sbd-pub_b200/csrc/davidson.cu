@@ -165,10 +165,15 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       // decided on the device) go back to back, and the step's scalars come back with its one
       // synchronisation.  If this step turns out converged, the extra work on t is discarded.
       const bool fast = !rec && !last && !(learned && cycle_mode == 1);
+      // a step of a learned cycle in the exchange-symmetric sector: the tile-pair residual now, the
+      // learned correction (or not) and the tile-pair Gram-Schmidt after the convergence test
+      const bool lsym = sym && !rec && !last && learned && cycle_mode == 1;
       double t0_fast = 0.0, tt_fast = 0.0;
       std::vector<double> coef(ib + 1);
       for (int k = 0; k <= ib; k++) coef[k] = f[k] * f[k];
-      if (fast && sym) {
+      if (lsym) {
+        TPB_CHECK(residual_sym_async<T>(h, ra, 0));
+      } else if (fast && sym) {
         // exchange-symmetric subspace: residual with the projection of t folded in and both
         // Gram-Schmidt rounds in tile-pair form (half the subspace bytes of the general passes)
         TPB_CHECK(residual_sym_async<T>(h, ra, 0));
@@ -252,13 +257,33 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         stop = true;
         break;
       }
-      if (use_learned)
+      if (lsym) {
+        // t is t_sym (slots 2.. hold S_k.t, 2+ib+1 t.t).  The learned factor depends on the spatial
+        // occupation and on H_ii, which is exchange-symmetric only up to rounding, and above the
+        // inference budget it corrects a capped subset of entries; so the corrected t is projected
+        // again and its overlaps with the subspace recomputed for the Gram-Schmidt rounds
+        const int t0_slot = 2 + ib + 1;
+        if (use_learned) {
+          TPB_CHECK(precond_apply<T>(h, learned, tnext, energy, std::sqrt(out[1]), out[2 + ib + 1]));
+          TPB_CHECK(symmetrize_dots<T>(h, tnext, cp.data(), ib + 1, 2));
+          nlearned++;
+        }
+        TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, 1, kCgsSlot));
+        TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, 0, kCgs2Slot,
+                                   t0_slot, kCgsSlot));
+        const double *sc2 = fetch_scalars(h, kScalarSlots);
+        if (!sc2) return SBD_TPB_ERR_CUDA;
+        t0_fast = sc2[t0_slot];
+        const double tt1 = sc2[kCgsSlot];
+        tt_fast = tt1 < 0.5 * t0_fast ? sc2[kCgs2Slot] : tt1;
+      }
+      if (use_learned && !lsym)
         TPB_CHECK(precond_apply<T>(h, learned, tnext, energy, std::sqrt(out[1]), out[2 + ib + 1]));
-      if (sym && !last && !fast) {
+      if (sym && !last && !fast && !lsym) {
         // the S_k are exactly symmetric, so S_k.t is unchanged by the projection; only t.t is
         TPB_CHECK(symmetrize<T>(h, tnext, &out[2 + ib + 1]));
       }
-      if (use_learned) {
+      if (use_learned && !lsym) {
         // overlaps S_k.t and t.t of the learned correction for the Gram-Schmidt below
         std::vector<const T *> xp(ib + 2);
         for (int k = 0; k <= ib; k++) xp[k] = S[k].p;
@@ -274,7 +299,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         // subspace to working precision).
         double t0 = t0_fast, tt = tt_fast;
         std::vector<double> o(ib + 1);
-        if (!fast) {  // (the fast path ran both rounds on the device)
+        if (!fast && !lsym) {  // (the fast and learned-cycle symmetric paths ran both rounds on the device)
           t0 = out[2 + ib + 1];
           for (int k = 0; k <= ib; k++) o[k] = f[k] * f[k] * out[2 + k];
           TPB_CHECK(cgs_update<T>(h, cp.data(), ib + 1, o.data(), tnext, n, 1, dots.data()));
@@ -303,7 +328,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
       }
       // max_time guard (tpb/davidson.h:887-913): stop when the next step would overrun (after the
       // fast path the stream is already idle)
-      if (!fast) TPB_CUDA(cudaStreamSynchronize(h->stream));
+      if (!fast && !lsym) TPB_CUDA(cudaStreamSynchronize(h->stream));
       const auto s1 = std::chrono::steady_clock::now();
       step_times.push_back(std::chrono::duration<double>(s1 - s0).count());
       double avg = 0.0;

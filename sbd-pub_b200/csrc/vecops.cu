@@ -355,17 +355,19 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(T *__restrict__ t, uint
 // block partials of S_k . t_new for k < m: S_k and the new t are exactly symmetric, so the (bj, bi)
 // tile of a pair repeats the (bi, bj) tile's products and each off-diagonal pair is counted twice
 // from its (bi, bj) tile (half the S_k bytes of a separate dot pass, and no second read of t).
-template <typename T, int VW>
+// kAvg: t <- (t + t^T) / 2 (the exchange projection) and partial m is t_new . t_new.
+template <typename T, int VW, bool kAvg = false>
 __global__ void __launch_bounds__(256)
     sym_add_dots_kernel(T *__restrict__ t, uint32_t nb, VecPtrs<T> S, int m, double *partials) {
   constexpr int TS = kSymTile, TPR = TS / VW, RS = 256 / TPR;
+  constexpr double kW = kAvg ? 0.5 : 1.0;
   __shared__ T A[TS][TS + 1], B[TS][TS + 1];
   const uint32_t nt = (nb + TS - 1) / TS;
   const size_t npairs = (size_t)nt * (nt + 1) / 2;
   const int cx = (threadIdx.x % TPR) * VW, ty = threadIdx.x / TPR;
-  double acc[kMaxSub];
+  double acc[kMaxSub + 1];
 #pragma unroll
-  for (int k = 0; k < kMaxSub; k++) acc[k] = 0.0;
+  for (int k = 0; k <= kMaxSub; k++) acc[k] = 0.0;
   for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
     uint32_t bi = (uint32_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
     while (bi > 0 && (size_t)bi * nt - (size_t)bi * (bi - 1) / 2 > p) bi--;
@@ -399,9 +401,15 @@ __global__ void __launch_bounds__(256)
       const uint32_t i = bi * TS + r, j = bj * TS + cx;
       T v[VW];
 #pragma unroll
-      for (int l = 0; l < VW; l++) v[l] = (T)((double)A[r][cx + l] + (double)B[cx + l][r]);
+      for (int l = 0; l < VW; l++) v[l] = (T)(((double)A[r][cx + l] + (double)B[cx + l][r]) * kW);
       if (i < nb && j < nb) {
         stv<T, VW>(t + (size_t)i * nb + j, v);
+        if (kAvg) {
+          double d = 0.0;
+#pragma unroll
+          for (int l = 0; l < VW; l++) d += (double)v[l] * (double)v[l];
+          acc[kMaxSub] += mult * d;
+        }
 #pragma unroll
         for (int k = 0; k < kMaxSub; k++) {
           if (k < m) {
@@ -421,12 +429,17 @@ __global__ void __launch_bounds__(256)
         const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
         T v[VW];
 #pragma unroll
-        for (int l = 0; l < VW; l++) v[l] = (T)((double)A[cx + l][r] + (double)B[r][cx + l]);
+        for (int l = 0; l < VW; l++) v[l] = (T)(((double)A[cx + l][r] + (double)B[r][cx + l]) * kW);
         if (i2 < nb && j2 < nb) stv<T, VW>(t + (size_t)i2 * nb + j2, v);
       }
     }
   }
-  block_reduce_store<kMaxSub>(acc, m, partials, gridDim.x);
+  if (kAvg) {
+#pragma unroll
+    for (int k = 0; k < kMaxSub; k++)
+      if (k == m) acc[k] = acc[kMaxSub];  // (acc[m] is unused: dots run over k < m)
+  }
+  block_reduce_store<kMaxSub + 1>(acc, kAvg ? m + 1 : m, partials, gridDim.x);
 }
 
 // Tile-pair forms of the Davidson step's vector passes for exchange-symmetric subspaces (every S_k
@@ -611,18 +624,19 @@ __global__ void __launch_bounds__(256)
 // it multiplies, and of the diagonal -- is issued before the first barrier, so a tile pair waits on one
 // round of memory latency instead of two or three (the general forms loaded the subspace tiles only
 // after the barrier and ran FP32 at ~3 TB/s).  Same arithmetic, same order per element.
-template <int M>
+template <int M, bool kAvg = false>
 __global__ void __launch_bounds__(256)
     sym_add_dots_f32_kernel(float *__restrict__ t, uint32_t nb, VecPtrs<float> S, double *partials) {
   constexpr int TS = kSymTile, VW = 4, TPR = TS / VW;
   static_assert(256 / TPR == TS, "one tile row per thread");
+  constexpr double kW = kAvg ? 0.5 : 1.0;
   __shared__ float A[TS][TS + 1], B[TS][TS + 1];
   const uint32_t nt = (nb + TS - 1) / TS;
   const size_t npairs = (size_t)nt * (nt + 1) / 2;
   const int cx = (threadIdx.x % TPR) * VW, r = threadIdx.x / TPR;
-  double acc[M];
+  double acc[M + 1];
 #pragma unroll
-  for (int k = 0; k < M; k++) acc[k] = 0.0;
+  for (int k = 0; k <= M; k++) acc[k] = 0.0;
   for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
     uint32_t bi, bj;
     tile_pair(p, nt, bi, bj);
@@ -650,7 +664,7 @@ __global__ void __launch_bounds__(256)
     if (in1) {
       float v[VW];
 #pragma unroll
-      for (int l = 0; l < VW; l++) v[l] = (float)((double)A[r][cx + l] + (double)B[cx + l][r]);
+      for (int l = 0; l < VW; l++) v[l] = (float)(((double)A[r][cx + l] + (double)B[cx + l][r]) * kW);
       stv<float, VW>(t + (size_t)i * nb + j, v);
 #pragma unroll
       for (int k = 0; k < M; k++) {
@@ -659,15 +673,21 @@ __global__ void __launch_bounds__(256)
         for (int l = 0; l < VW; l++) d += (double)v[l] * (double)sv[k][l];
         acc[k] += mult * d;
       }
+      if (kAvg) {
+        double d = 0.0;
+#pragma unroll
+        for (int l = 0; l < VW; l++) d += (double)v[l] * (double)v[l];
+        acc[M] += mult * d;
+      }
     }
     if (bi != bj && in2) {
       float v[VW];
 #pragma unroll
-      for (int l = 0; l < VW; l++) v[l] = (float)((double)A[cx + l][r] + (double)B[r][cx + l]);
+      for (int l = 0; l < VW; l++) v[l] = (float)(((double)A[cx + l][r] + (double)B[r][cx + l]) * kW);
       stv<float, VW>(t + (size_t)i2 * nb + j2, v);
     }
   }
-  block_reduce_store<M>(acc, M, partials, gridDim.x);
+  block_reduce_store<M + 1>(acc, kAvg ? M + 1 : M, partials, gridDim.x);
 }
 
 template <int M>
@@ -750,6 +770,204 @@ __global__ void __launch_bounds__(256)
       stv<float, VW>(a.t + (size_t)i2 * nb + j2, v);
     }
   }
+  block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
+}
+
+// 16-byte asynchronous global -> shared copy (zero fill when !valid; gmem must still be a valid
+// address), its commit and wait
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The tile-pair residual pass as a two-stage pipeline: while a block computes one tile pair from
+// shared memory, the copies of its next pair (the (bi, bj) tiles of every C_k and sigma(S_k) and of
+// the stored diagonal, and the (bj, bi) tile of the diagonal) are in flight, so the bytes in flight
+// do not live in registers (the register forms hold one pair: the FP32 one ran one block per SM and
+// ~2.7 TB/s at M = 6..8).  Each thread copies and later reads back only its own 16-byte chunks,
+// except for the transposed diagonal tile, which every thread reads across the tile after a
+// barrier; its chunks are XOR-swizzled by row so those reads spread over the banks.  The block
+// walks its tile pairs incrementally (one square root per block, not per pair and thread).
+//
+// Arithmetic, chosen for instruction count (the register forms issued ~280 instructions per
+// element, most of them FP32<->FP64 conversions, which run at a quarter of the FP64 rate, and two
+// FP64 divisions): W = sum u_k C_k, sum u_k sigma_k, r = E' W - sum u_k sigma_k, W.W and r.r in
+// FP64 (r cancels), then t_sym = r (1/(E0 - H_ij) + 1/(E0 - H_ji)) / 2 as r (d1 + d2) / (2 d1 d2),
+// one division, in the vector type (FP32 vectors: FP32, from r rounded to FP32 and
+// E0 - H = (E'_hi - H') + E'_lo; each d with the reference's 1e-12 regularisation), and the
+// overlaps S_k . t_sym and t_sym . t_sym from per-thread partial sums of four FP32 products that are
+// added in FP64.  t differs from the register forms' in its last bits only.  Used while both stages
+// fit in shared memory (FP32 up to M = 8, FP64 up to 5).
+template <typename T, int M>
+constexpr size_t residual_pipe_smem() {
+  return (2 * (size_t)(2 * M + 2) * kSymTile * kSymTile + (size_t)kSymTile * (kSymTile + 1)) * sizeof(T);
+}
+template <typename T>
+constexpr int residual_pipe_max() {
+  return sizeof(T) == 4 ? 8 : 5;
+}
+static_assert(residual_pipe_smem<float, residual_pipe_max<float>()>() <= 227 * 1024, "FP32 stages");
+static_assert(residual_pipe_smem<double, residual_pipe_max<double>()>() <= 227 * 1024, "FP64 stages");
+// (bi, bj) of the tile pair `step` positions further in the row-major upper triangle
+__device__ __forceinline__ void tile_pair_advance(uint32_t nt, uint32_t step, uint32_t &bi, uint32_t &bj) {
+  uint32_t off = bj - bi + step;
+  while (bi < nt && off >= nt - bi) {
+    off -= nt - bi;
+    bi++;
+  }
+  bj = bi + off;
+}
+template <typename T, int M>
+__global__ void __launch_bounds__(256)
+    residual_sym_pipe_kernel(ResidualArgs<T> a, uint32_t nb, double *partials) {
+  constexpr int TS = kSymTile, VW = 16 / sizeof(T), CPR = TS / VW;  // chunks per tile row
+  constexpr int NCH = TS * CPR / 256;                                 // chunks of a tile per thread
+  constexpr int RS = 256 / CPR;                                       // rows between a thread's chunks
+  constexpr int kTile = TS * TS, kStage = (2 * M + 2) * kTile;
+  constexpr bool kF32 = sizeof(T) == 4;
+  static_assert(CPR >= 8 && NCH * 256 == TS * CPR, "tile of whole 16-byte chunks");
+  extern __shared__ __align__(16) unsigned char psm_raw[];
+  T *psm = reinterpret_cast<T *>(psm_raw);
+  T(*Tt)[TS + 1] = reinterpret_cast<T(*)[TS + 1]>(psm + 2 * kStage);
+  if (a.u_dev) {
+#pragma unroll
+    for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
+    a.e_shifted = __ldg(&a.e_dev[0]);
+    a.e0 = a.e_shifted + a.shift;
+  }
+  // E0 - H_ii: from H_ii - H_00 (FP32, against E0 - H_00 split in two floats) or from H_ii (FP64)
+  const float e_hi = (float)a.e_shifted, e_lo = (float)(a.e_shifted - (double)e_hi);
+  const T *hsrc = kF32 ? reinterpret_cast<const T *>(a.hii32) : reinterpret_cast<const T *>(a.hii);
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int q = threadIdx.x % CPR, cx = q * VW, ty = threadIdx.x / CPR;
+  auto issue = [&](uint32_t bi, uint32_t bj, T *st) {
+#pragma unroll
+    for (int hh = 0; hh < NCH; hh++) {
+      const int r = ty + hh * RS;
+      const uint32_t i = bi * TS + r, j = bj * TS + cx, i2 = bj * TS + r, j2 = bi * TS + cx;
+      const bool in1 = i < nb && j < nb, in2 = i2 < nb && j2 < nb;
+      const size_t base = in1 ? (size_t)i * nb + j : 0, base2 = in2 ? (size_t)i2 * nb + j2 : 0;
+      const int own = r * TS + cx, own_sw = r * TS + ((q ^ ((r / VW) & 7)) * VW);
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        cp_async16(st + k * kTile + own, a.C.p[k] + base, in1);
+        cp_async16(st + (M + k) * kTile + own, a.HC.p[k] + base, in1);
+      }
+      cp_async16(st + 2 * M * kTile + own, hsrc + base, in1);
+      cp_async16(st + (2 * M + 1) * kTile + own_sw, hsrc + base2, in2);
+    }
+  };
+  double acc[M + 3];
+#pragma unroll
+  for (int k = 0; k < M + 3; k++) acc[k] = 0.0;
+  int s = 0;
+  uint32_t bi = 0, bj = 0;
+  if (blockIdx.x < npairs) {
+    tile_pair(blockIdx.x, nt, bi, bj);
+    issue(bi, bj, psm);
+  }
+  cp_async_commit();
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x, s ^= 1) {
+    uint32_t nbi = bi, nbj = bj;
+    tile_pair_advance(nt, gridDim.x, nbi, nbj);
+    if (p + gridDim.x < npairs) issue(nbi, nbj, psm + (s ^ 1) * kStage);
+    cp_async_commit();
+    cp_async_wait<1>();  // this pair's copies (this thread's) have landed
+    __syncthreads();     // ... and every thread's, for the transposed diagonal tile
+    const T *st = psm + s * kStage;
+    const double mult = bi == bj ? 1.0 : 2.0;
+#pragma unroll
+    for (int hh = 0; hh < NCH; hh++) {
+      const int r = ty + hh * RS, own = r * TS + cx;
+      const uint32_t i = bi * TS + r, j = bj * TS + cx;
+      if (i >= nb || j >= nb) continue;
+      double w[VW], hc[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) w[l] = hc[l] = 0.0;
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+#pragma unroll
+        for (int l = 0; l < VW; l++) {
+          w[l] += a.u[k] * (double)st[k * kTile + own + l];
+          hc[l] += a.u[k] * (double)st[(M + k) * kTile + own + l];
+        }
+      }
+      // the transposed entry (j + l, i): row cx + l, column r of the swizzled tile
+      const T *ht = st + (2 * M + 1) * kTile + (((r / VW) ^ (q & 7)) * VW) + (r % VW);
+      T v[VW];
+      double ww = 0.0, rr = 0.0;
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        const double rv = a.e_shifted * w[l] - hc[l];
+        ww += w[l] * w[l];
+        rr += rv * rv;
+        const T h1 = st[2 * M * kTile + own + l], h2 = ht[(cx + l) * TS];
+        if constexpr (kF32) {
+          float d1 = (e_hi - (float)h1) + e_lo, d2 = (e_hi - (float)h2) + e_lo;
+          d1 = fabsf(d1) > 1.0e-12f ? d1 : d1 - 1.0e-12f;
+          d2 = fabsf(d2) > 1.0e-12f ? d2 : d2 - 1.0e-12f;
+          v[l] = (T)(0.5f * (float)rv * (d1 + d2) / (d1 * d2));
+        } else {
+          double d1 = a.e0 - (double)h1, d2 = a.e0 - (double)h2;
+          d1 = fabs(d1) > 1.0e-12 ? d1 : d1 - 1.0e-12;
+          d2 = fabs(d2) > 1.0e-12 ? d2 : d2 - 1.0e-12;
+          v[l] = (T)(0.5 * rv * (d1 + d2) / (d1 * d2));
+        }
+        Tt[r][cx + l] = v[l];
+      }
+      acc[0] += mult * ww;
+      acc[1] += mult * rr;
+      if constexpr (kF32) {
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+          float pk = 0.f;
+#pragma unroll
+          for (int l = 0; l < VW; l++) pk = fmaf((float)st[k * kTile + own + l], (float)v[l], pk);
+          acc[2 + k] += mult * (double)pk;
+        }
+        float vv = 0.f;
+#pragma unroll
+        for (int l = 0; l < VW; l++) vv = fmaf((float)v[l], (float)v[l], vv);
+        acc[2 + M] += mult * (double)vv;
+      } else {
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+          double pk = 0.0;
+#pragma unroll
+          for (int l = 0; l < VW; l++) pk += (double)st[k * kTile + own + l] * (double)v[l];
+          acc[2 + k] += mult * pk;
+        }
+        double vv = 0.0;
+#pragma unroll
+        for (int l = 0; l < VW; l++) vv += (double)v[l] * (double)v[l];
+        acc[2 + M] += mult * vv;
+      }
+      stv<T, VW>(a.t + (size_t)i * nb + j, v);
+    }
+    __syncthreads();
+    if (bi != bj) {
+#pragma unroll
+      for (int hh = 0; hh < NCH; hh++) {
+        const int r = ty + hh * RS;
+        const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
+        if (i2 >= nb || j2 >= nb) continue;
+        T v[VW];
+#pragma unroll
+        for (int l = 0; l < VW; l++) v[l] = Tt[cx + l][r];
+        stv<T, VW>(a.t + (size_t)i2 * nb + j2, v);
+      }
+    }
+    bi = nbi;
+    bj = nbj;
+  }
+  cp_async_wait<0>();
   block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
 }
 
@@ -1090,8 +1308,9 @@ int sym_add(sbd_tpb_handle *h, T *x) {
   return SBD_TPB_OK;
 }
 
-template <typename T>
-int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
+// kAvg: x <- (x + x^T) / 2 and x.x after S_k.x (m + 1 slots from `slot`)
+template <typename T, bool kAvg>
+static int sym_dots_impl(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
   if (m < 1 || m > kMaxSub) return fail(SBD_TPB_ERR_INVALID, "subspace larger than supported");
   TPB_CHECK(ensure_scalars(h));
   const uint32_t nb = (uint32_t)h->bstr.size();
@@ -1107,19 +1326,28 @@ int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
     TPB_CHECK(dispatch_n<1>(m, [&](auto K) {
       constexpr int M = decltype(K)::value;
       if constexpr (M <= kMaxSub) {
-        sym_add_dots_f32_kernel<M><<<nblk, 256, 0, h->stream>>>(reinterpret_cast<float *>(x), nb,
-                                                                 *reinterpret_cast<VecPtrs<float> *>(&P),
-                                                                 h->d_partials);
+        sym_add_dots_f32_kernel<M, kAvg><<<nblk, 256, 0, h->stream>>>(
+            reinterpret_cast<float *>(x), nb, *reinterpret_cast<VecPtrs<float> *>(&P), h->d_partials);
         TPB_LAUNCHED(h);
       }
       return SBD_TPB_OK;
     }));
   } else {
-    if (vec) sym_add_dots_kernel<T, VW><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
-    else sym_add_dots_kernel<T, 1><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+    if (vec) sym_add_dots_kernel<T, VW, kAvg><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
+    else sym_add_dots_kernel<T, 1, kAvg><<<nblk, 256, 0, h->stream>>>(x, nb, P, m, h->d_partials);
     TPB_LAUNCHED(h);
   }
-  return reduce_into(h, m, h->d_scal + slot, nblk);
+  return reduce_into(h, kAvg ? m + 1 : m, h->d_scal + slot, nblk);
+}
+
+template <typename T>
+int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
+  return sym_dots_impl<T, false>(h, x, S, m, slot);
+}
+
+template <typename T>
+int symmetrize_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot) {
+  return sym_dots_impl<T, true>(h, x, S, m, slot);
 }
 
 template <typename T>
@@ -1148,21 +1376,32 @@ int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
   }
   ptrs[np++] = a.t;
   const bool vec = pair_vec_ok<T>(nb, ptrs, np);
+  int grid = nblk;
   TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
     constexpr int M = decltype(K)::value;
     if constexpr (M <= kMaxSub) {
-      if constexpr (sizeof(T) == 4) {
-        if (vec) residual_sym_f32_kernel<M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
-        else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      constexpr bool kPipe = M <= residual_pipe_max<T>();
+      constexpr int MP = kPipe ? M : 1;
+      constexpr size_t smem = residual_pipe_smem<T, MP>();
+      if (vec && kPipe && smem <= h->smem_optin) {
+        const auto kern = residual_sym_pipe_kernel<T, MP>;
+        TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        TPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+        grid = h->num_sms * std::max(1, std::min(per_sm, kSymBlocksPerSm));
+        kern<<<grid, 256, smem, h->stream>>>(a, nb, h->d_partials);
+      } else if (!vec) {
+        residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      } else if constexpr (sizeof(T) == 4) {
+        residual_sym_f32_kernel<M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
       } else {
-        if (vec) residual_sym_kernel<T, 16 / sizeof(T), M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
-        else residual_sym_kernel<T, 1, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+        residual_sym_kernel<T, 16 / sizeof(T), M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
       }
       TPB_LAUNCHED(h);
     }
     return SBD_TPB_OK;
   }));
-  return reduce_into(h, a.m + 3, h->d_scal + slot, nblk);
+  return reduce_into(h, a.m + 3, h->d_scal + slot, grid);
 }
 
 template <typename T>
@@ -1231,6 +1470,8 @@ template int cgs_second_round_async<float>(sbd_tpb_handle *, const float *const 
                                            float *, size_t, int, int, int);
 template int sym_add_dots<double>(sbd_tpb_handle *, double *, const double *const *, int, int);
 template int sym_add_dots<float>(sbd_tpb_handle *, float *, const float *const *, int, int);
+template int symmetrize_dots<double>(sbd_tpb_handle *, double *, const double *const *, int, int);
+template int symmetrize_dots<float>(sbd_tpb_handle *, float *, const float *const *, int, int);
 template int residual_sym_async<double>(sbd_tpb_handle *, const ResidualArgs<double> &, int);
 template int residual_sym_async<float>(sbd_tpb_handle *, const ResidualArgs<float> &, int);
 template int cgs_sym_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, int, double *, int,

@@ -62,6 +62,10 @@ int cgs_sym_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coe
 // the same, and S_k . x_new (k < m, S_k exactly symmetric) into scalar slots slot..
 template <typename T>
 int sym_add_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot);
+// x <- (x + x^T) / 2 (the exchange projection), S_k . x_new into slots slot .. slot+m-1 and x_new . x_new
+// into slot+m, in one tile-pair pass
+template <typename T>
+int symmetrize_dots(sbd_tpb_handle *h, T *x, const T *const *S, int m, int slot);
 
 // The same passes without a host round trip: each reduces into slots of a small device array
 // (kScalarSlots doubles), read back together by fetch_scalars (one stream synchronisation).
