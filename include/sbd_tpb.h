@@ -69,7 +69,10 @@ typedef struct sbd_tpb_params {
   int max_nb;        /* --block: subspace size (default 10) */
   double eps;        /* --tolerance: residual norm (default 1e-4) */
   double max_time;   /* --max_time in seconds (default 86400) */
-  int init;          /* --init: 0 = start from determinant 0 (the reference's HF start) */
+  int init;          /* --init: 0 = start from determinant 0 (the reference's HF start);
+                        1 = the reference's seeded random start (BasisInitVector with init 1,
+                        tpb/davidson.h:138-141: Randomize, framework/dm_vector.h:101-178, the same
+                        values for the same seed, normalised) */
   int do_rdm;        /* --rdm: 0 = orbital occupations only, 1 = full 1/2-RDMs */
   int precision;     /* SBD_TPB_FP64 or SBD_TPB_MIXED */
   int preconditioner;/* SBD_TPB_PRECOND_* */
@@ -79,8 +82,12 @@ typedef struct sbd_tpb_params {
                         start is the HF determinant, every correction vector is projected onto
                         the alpha<->beta exchange-symmetric sector the start vector lies in
                         (C = C^T in the separated convention), so rounding cannot steer the
-                        iteration to a lower state of the other sector; 0: off */
+                        iteration to a lower state of the other sector; 2: the same, and a
+                        random start (init 1) is projected onto that sector too (the reference
+                        does not project; its random start reaches the lowest state of either
+                        sector); 0: off.  Davidson only. */
   int method;        /* --method: SBD_TPB_METHOD_DAVIDSON (default) or SBD_TPB_METHOD_LANCZOS */
+  unsigned long long seed; /* --seed of the random start (default 1729, tpb/sbdiag.h:34) */
 } sbd_tpb_params;
 
 /* Fills p with the reference defaults (tpb/sbdiag.h:22-50) and SBD_TPB_FP64 / diagonal. */

@@ -58,7 +58,7 @@ inline void diag(const MPI_Comm &comm, const sbd::tpb::SBD &s, const sbd::FCIDum
     throw std::runtime_error("sbd_b200::diag runs one rank on one GPU");
   if (s.method != SBD_TPB_METHOD_DAVIDSON && s.method != SBD_TPB_METHOD_LANCZOS)
     throw std::runtime_error("sbd_b200::diag: --method 0 (Davidson) or 2 (Lanczos) only");
-  if (s.init != 0) throw std::runtime_error("sbd_b200::diag: --init 0 only");
+  if (s.init != 0 && s.init != 1) throw std::runtime_error("sbd_b200::diag: --init 0 or 1 only");
 
   // the Hamiltonian as SetupIntegrals builds it (framework/makeintegrals.h:123-174): I1 over spin
   // orbitals (the alpha block is the spatial matrix), I2 as the 8-fold packed store
@@ -79,6 +79,7 @@ inline void diag(const MPI_Comm &comm, const sbd::tpb::SBD &s, const sbd::FCIDum
   p.eps = s.eps;
   p.max_time = s.max_time;
   p.init = s.init;
+  p.seed = s.seed;
   p.do_rdm = s.do_rdm;
   p.method = s.method;
   p.device = device;
@@ -87,7 +88,8 @@ inline void diag(const MPI_Comm &comm, const sbd::tpb::SBD &s, const sbd::FCIDum
   const size_t ndet = a.size() * b.size();
 
   // start vector: the reference's restart file when asked for (W in the reference's order and sign
-  // convention, as sbd_tpb_diag_from takes it), else the HF determinant
+  // convention, as sbd_tpb_diag_from takes it), else the start --init selects (HF determinant or
+  // the seeded random vector, both built by the library)
   MPI_Comm h_comm, b_comm, t_comm, a_comm;
   sbd::TaskCommunicator(comm, 1, 1, 1, 1, h_comm, b_comm, t_comm, a_comm);
   std::vector<double> W0;

@@ -183,6 +183,24 @@ def hash_vector(idx) -> np.ndarray:
     return ((i * np.uint64(0x9E3779B97F4A7C15)) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53 - 0.5
 
 
+def random_start(n: int, seed: int, normalise: bool = True) -> np.ndarray:
+    """The reference's seeded random start (BasisInitVector with init 1, tpb/davidson.h:138-141):
+    element i = uniform in [-1, 1) from the splitmix64-style mix of (seed, i) of Randomize
+    (framework/dm_vector.h:100-178), in the reference's determinant order and sign convention;
+    normalised to unit length when asked (the reference's norm is a Kahan sum per thread, so its
+    last bit can differ)."""
+    i = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) * np.uint64(6364136223846793005) + i * np.uint64(2862933555777941757)
+        x ^= x >> np.uint64(30)
+        x *= np.uint64(0xBF58476D1CE4E5B9)
+        x ^= x >> np.uint64(27)
+        x *= np.uint64(0x94D049BB133111EB)
+        x ^= x >> np.uint64(31)
+    w = (x >> np.uint64(11)).astype(np.float64) * (2.0 / 9007199254740992.0) - 1.0
+    return w / np.sqrt(np.dot(w, w)) if normalise else w
+
+
 class System:
     """Strings + Hamiltonian + tables: the oracle's view of one TPB problem."""
 

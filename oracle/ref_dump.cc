@@ -14,8 +14,9 @@
 //                         (--sigma_seed: normal deviates; --sigma_hash: the closed-form vector
 //                         x_i = ((i * 0x9E3779B97F4A7C15 mod 2^64) >> 11) / 2^53 - 1/2, which a
 //                         test regenerates exactly at any size without storing it)
-//   davidson.txt / W.f64  Davidson (tpb/davidson.h:667-930) from the HF start, energy as in
-//                         tpb/sbdiag.h:431-469
+//   davidson.txt / W.f64  Davidson (tpb/davidson.h:667-930) from the HF start (--init 0) or the
+//                         seeded random start (--init 1 SEED: BasisInitVector, tpb/davidson.h:138-141,
+//                         whose vector is also written as w0.f64), energy as in tpb/sbdiag.h:431-469
 //   rdm1.f64 / rdm2.f64   Correlation (tpb/correlation.h:378-664)
 //   lanczos.txt / W_lanczos.f64   Lanczos (tpb/lanczos.h:167-320) from the HF start: energy
 //                         <W|H|W> (as tpb/sbdiag.h:431-469) and the final vector
@@ -31,7 +32,7 @@
 //                         trailing strings (a null dereference in MpiBcast)
 //
 // Usage: ref_dump --fcidump F --adetfile A [--bdetfile B] [--bit_length 20] --out DIR
-//                 [--sigma_seed S | --sigma_hash] [--davidson IT NB TOL] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
+//                 [--sigma_seed S | --sigma_hash] [--davidson IT NB TOL] [--init I SEED] [--rdm] [--carryover RATIO THRESHOLD CUTOFF]
 //                 [--lanczos IT NB TOL]
 // The reference headers rely on their includer for these (as its app main.cc does).
 #include <chrono>
@@ -96,7 +97,8 @@ int main(int argc, char **argv) {
   size_t bit_length = 20;
   long sigma_seed = -1;
   bool sigma_hash = false;
-  int dav_it = 0, dav_nb = 0;
+  int dav_it = 0, dav_nb = 0, dav_init = 0;
+  unsigned long long dav_seed = 1729;
   double dav_tol = 1e-8;
   bool do_rdm = false;
   double co_ratio = -1.0, co_threshold = 0.0, co_cutoff = 0.0;
@@ -115,6 +117,9 @@ int main(int argc, char **argv) {
       dav_it = std::atoi(argv[++i]);
       dav_nb = std::atoi(argv[++i]);
       dav_tol = std::atof(argv[++i]);
+    } else if (a == "--init") {
+      dav_init = std::atoi(argv[++i]);
+      dav_seed = std::strtoull(argv[++i], nullptr, 10);
     } else if (a == "--rdm") do_rdm = true;
     else if (a == "--lanczos") {
       lz_it = std::atoi(argv[++i]);
@@ -209,7 +214,8 @@ int main(int argc, char **argv) {
 
   if (dav_it > 0) {
     std::vector<double> W;
-    sbd::BasisInitVector(W, adet, bdet, 1, 1, h_comm, b_comm, t_comm, 0, 1729);
+    sbd::BasisInitVector(W, adet, bdet, 1, 1, h_comm, b_comm, t_comm, dav_init, dav_seed);
+    if (dav_init != 0) write_raw(out + "/w0.f64", W.data(), W.size());
     sbd::Davidson(hii, W, adet, bdet, bit_length, static_cast<size_t>(L), 1, 1, helper, I0, I1, I2,
                   h_comm, b_comm, t_comm, dav_it, dav_nb, dav_tol, 86400.0);
     std::vector<double> C(W.size(), 0.0);

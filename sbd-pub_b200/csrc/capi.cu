@@ -87,6 +87,7 @@ void sbd_tpb_default_params(sbd_tpb_params *p) {
   p->device = 0;
   p->symmetry = 1;
   p->method = SBD_TPB_METHOD_DAVIDSON;
+  p->seed = 1729;
 }
 
 const char *sbd_tpb_last_error(void) { return g_last_error.c_str(); }
@@ -353,6 +354,7 @@ int sbd_tpb_davidson(sbd_tpb_handle *h, const sbd_tpb_params *params, const doub
   TPB_HANDLE(h);
   if (!params || !result) return fail(SBD_TPB_ERR_INVALID, "null params/result");
   if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
+  if (params->init != 0 && params->init != 1) return fail(SBD_TPB_ERR_INVALID, "init must be 0 or 1");
   return davidson_run(h, params, W0, result);
 }
 
@@ -361,6 +363,7 @@ int sbd_tpb_lanczos(sbd_tpb_handle *h, const sbd_tpb_params *params, const doubl
   TPB_HANDLE(h);
   if (!params || !result) return fail(SBD_TPB_ERR_INVALID, "null params/result");
   if (!h->have_tables) return fail(SBD_TPB_ERR_STATE, "tables not built");
+  if (params->init != 0 && params->init != 1) return fail(SBD_TPB_ERR_INVALID, "init must be 0 or 1");
   return lanczos_run(h, params, W0, result);
 }
 

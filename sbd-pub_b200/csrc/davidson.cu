@@ -40,6 +40,13 @@ namespace {
 // device skipped it), [44, 44+ib+1) overlaps S_k . sigma(S_ib), [60, 64) the lowest Ritz values.
 constexpr int kSymSlot = 20, kCgsSlot = 24, kCgs2Slot = 41, kOvSlot = 44, kEigSlot = 60;
 
+// alpha <-> beta exchange symmetry (C = C^T): the HF start lies in the symmetric sector and H
+// preserves it, so corrections are projected back onto it (and, with symmetry 2, the random start
+// is projected onto it first); every vector of such a run is exactly symmetric
+bool symmetric_run(const sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0) {
+  return !W0 && h->astr == h->bstr && (prm->symmetry == 2 || (prm->symmetry == 1 && prm->init == 0));
+}
+
 template <typename T>
 int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, double shift,
               double *dWout, double *resid_out, int *nsigma_out, int *converged_out, DavRecord *rec,
@@ -64,6 +71,16 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
     if (W0) {
       TPB_CUDA(cudaMemcpyAsync(dWout, W0, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
       TPB_CHECK(reorder_sign_apply_f64(h, dWout, dWout));
+    } else if (prm->init == 1) {
+      // --init 1: the reference's seeded random vector (tpb/davidson.h:138-141); its normalisation
+      // is the scale factor f_0 below.  With symmetry 2 it is projected onto the exchange-symmetric
+      // sector first (in the separated convention, (x + x^T) / 2).
+      TPB_CHECK(random_start_vector(h, dWout, n, prm->seed));
+      TPB_CHECK(reorder_sign_apply_f64(h, dWout, dWout));
+      if (prm->symmetry == 2 && h->astr == h->bstr) {
+        double tt = 0.0;
+        TPB_CHECK(symmetrize<double>(h, dWout, &tt));
+      }
     } else {
       // --init 0: the first determinant, i.e. the HF string when it is the smallest
       // (tpb/davidson.h:134-137)
@@ -88,10 +105,7 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
   double norm_R = 0.0, ww = 1.0;
   int nsigma = 0, m_last = 0;
   bool converged = false, stop = false, w_current = false;
-  // alpha <-> beta exchange symmetry (C = C^T): the HF start lies in the symmetric sector and
-  // H preserves it, so corrections are projected back onto it (rounding would otherwise let the
-  // iteration drift to a lower state of the antisymmetric sector)
-  const bool sym = prm->symmetry && !W0 && h->astr == h->bstr;
+  const bool sym = symmetric_run(h, prm, W0);
   ResidualArgs<T> ra;
   double energy = 0.0, prev_norm = 0.0;
   bool prev_learned = false;
@@ -180,6 +194,8 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
         TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), 2, tnext, 1, kCgsSlot));
         TPB_CHECK(cgs_sym_async<T>(h, cp.data(), ib + 1, coef.data(), kCgsSlot + 1, tnext, 0, kCgs2Slot,
                                    2 + ib + 1, kCgsSlot));
+      } else if (sym && last) {
+        TPB_CHECK(residual_w_sym_async<T>(h, ra, 0));
       } else {
         TPB_CHECK(residual_step_async<T>(h, ra, n, 0));
         if (fast) {
@@ -347,8 +363,15 @@ int run_typed(sbd_tpb_handle *h, const sbd_tpb_params *prm, const double *W0, do
     ra.W = Wv.p;
     ra.t = nullptr;
     ra.m = m_last;
-    TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
-    ww = out[0];
+    if (sym) {
+      TPB_CHECK(residual_w_sym_async<T>(h, ra, 0));
+      const double *sc = fetch_scalars(h, kScalarSlots);
+      if (!sc) return SBD_TPB_ERR_CUDA;
+      ww = sc[0];
+    } else {
+      TPB_CHECK(residual_step<T>(h, ra, n, out.data()));
+      ww = out[0];
+    }
   }
   // W normalised and promoted to FP64 into dWout
   if (std::is_same<T, double>::value) {
@@ -402,17 +425,23 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
   }
   res->learned_steps = nl;
   res->fallback_steps = nf;
-  return solve_finish(h, dW.p, res, t0, nsig, conv, p->precision == SBD_TPB_MIXED ? -1.0 : resid);
+  return solve_finish(h, dW.p, res, t0, nsig, conv, p->precision == SBD_TPB_MIXED ? -1.0 : resid,
+                      symmetric_run(h, p, W0));
 }
 
 int solve_finish(sbd_tpb_handle *h, double *dW, sbd_tpb_result *res,
-                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid) {
+                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid, bool sym_w) {
   const size_t n = h->ndet();
-  // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|
+  // final FP64 sigma: energy <W|H|W> (tpb/sbdiag.h:431-469) and the FP64 residual |HW - E W|;
+  // the one-pass symmetric form when W is exactly exchange-symmetric
   DevVec<double> dHW;
   TPB_CHECK(dHW.get(h, n));
   double E = 0.0, rr = 0.0;
-  TPB_CHECK(sigma_sep<double>(h, dW, dHW.p, 0));
+  if (sym_w) {
+    TPB_CHECK(sigma_sep_sym<double>(h, dW, dHW.p, 0.0));
+  } else {
+    TPB_CHECK(sigma_sep<double>(h, dW, dHW.p, 0));
+  }
   const double *wp[1] = {dW};
   TPB_CHECK(multi_dot<double>(h, wp, 1, dHW.p, n, &E));
   TPB_CHECK(axpby<double>(h, dW, dHW.p, -E, 1.0, n));

@@ -195,11 +195,20 @@ int lanczos_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0, sb
   TPB_CHECK(HC.get(h, n));
   for (int k = 0; k < nb; k++) TPB_CHECK(C[k].get(h, n));
 
-  // start: the stored vector (reference convention in, separated inside) or the first determinant
-  // (BasisInitVector with init 0, tpb/davidson.h:134-137); no normalisation, as in the reference
+  // start: the stored vector (reference convention in, separated inside), the first determinant
+  // (BasisInitVector with init 0, tpb/davidson.h:134-137; no normalisation, as in the reference) or
+  // the seeded random vector, normalised (init 1, tpb/davidson.h:138-141)
   if (W0) {
     TPB_CUDA(cudaMemcpyAsync(W.p, W0, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
     TPB_CHECK(reorder_sign_apply_f64(h, W.p, W.p));
+  } else if (p->init == 1) {
+    TPB_CHECK(random_start_vector(h, W.p, n, p->seed));
+    TPB_CHECK(reorder_sign_apply_f64(h, W.p, W.p));
+    const double *wp[1] = {W.p};
+    double nrm = 0.0;
+    TPB_CHECK(multi_dot<double>(h, wp, 1, W.p, n, &nrm));
+    if (!(nrm > 0.0)) return fail(SBD_TPB_ERR_INVALID, "initial vector is zero");
+    TPB_CHECK(scale_vec<double>(h, W.p, 1.0 / std::sqrt(nrm), n));
   } else {
     TPB_CUDA(cudaMemsetAsync(W.p, 0, sizeof(double) * n, h->stream));
     const double one = 1.0;

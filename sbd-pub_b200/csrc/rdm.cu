@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kRdmThreads)
   for (uint32_t ib = threadIdx.x; ib < nbp; ib += blockDim.x) {
     const bool in = ib < nb;
     const double w = in ? W[(size_t)ia * nb + ib] : 0.0;
-    const double w2 = w * w;
+    const double w2 = __dmul_rn(w, w);  // rounded product (never fused): rdm_rowsum_kernel repeats it
     const uint64_t occ = in ? bstr[ib] : 0ull;
     s += w2;
     const unsigned lo = (unsigned)occ, hi = (unsigned)(occ >> 32);
@@ -95,6 +95,22 @@ __global__ void __launch_bounds__(kRdmThreads)
     for (int w = 0; w < kRdmThreads / 32; w++) v += mq[w][q];
     Y[(size_t)ia * L + q] = v;
   }
+}
+
+// rho_a[Ia] = sum_Ib W[Ia, Ib]^2 alone (orbital occupations need no pair sums): the same
+// per-thread order and block sum as rdm_row_kernel's rho_a, so the occupations repeat bit for bit
+__global__ void __launch_bounds__(kRdmThreads)
+    rdm_rowsum_kernel(const double *__restrict__ W, uint32_t nb, double *__restrict__ rho_a) {
+  __shared__ double red[32];
+  const uint32_t ia = blockIdx.x;
+  double s = 0.0;
+  const uint32_t nbp = (nb + 31) & ~31u;
+  for (uint32_t ib = threadIdx.x; ib < nbp; ib += blockDim.x) {
+    const double w = ib < nb ? W[(size_t)ia * nb + ib] : 0.0;
+    s += __dmul_rn(w, w);
+  }
+  const double t = block_sum(s, red);
+  if (threadIdx.x == 0) rho_a[ia] = t;
 }
 
 // Mpart[c][p*L + q] = sum over alpha rows Ia of chunk c with p in Ia of Y[Ia][q]
@@ -322,10 +338,42 @@ int rdm_sep(sbd_tpb_handle *h, const double *W, double *one, double *two, double
   const uint32_t na = (uint32_t)h->astr.size(), nb = (uint32_t)h->bstr.size();
   const int L = h->L;
   const size_t n = h->ndet();
-  Rdm R(L);
-  // ---- diagonal part (deterministic: fixed summation order throughout)
   constexpr uint32_t kChunk = 1024;
   const uint32_t nca = (na + kChunk - 1) / kChunk;
+  if (!one && !two) {
+    // orbital occupations only: the string weights rho (row and column sums of W^2), summed over
+    // each string's orbitals in the order the full pass below adds them
+    if (!density) return SBD_TPB_OK;
+    double *d_rho = nullptr, *d_cp = nullptr;
+    TPB_CUDA(cudaMalloc(&d_rho, sizeof(double) * ((size_t)na + nb)));
+    TPB_CUDA(cudaMalloc(&d_cp, sizeof(double) * (size_t)nca * nb));
+    rdm_rowsum_kernel<<<na, kRdmThreads, 0, h->stream>>>(W, nb, d_rho);
+    TPB_LAUNCHED(h);
+    dim3 gridc((nb + 255) / 256, nca);
+    rdm_colsum_kernel<<<gridc, 256, 0, h->stream>>>(W, na, nb, kChunk, d_cp);
+    TPB_LAUNCHED(h);
+    rdm_chunk_sum_kernel<<<(nb + 255) / 256, 256, 0, h->stream>>>(d_cp, nca, nb, d_rho + na);
+    TPB_LAUNCHED(h);
+    std::vector<double> rho((size_t)na + nb);
+    const cudaError_t e1 = cudaMemcpyAsync(rho.data(), d_rho, sizeof(double) * rho.size(), cudaMemcpyDeviceToHost,
+                                           h->stream);
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamSynchronize(h->stream) : e1;
+    cudaFree(d_rho);
+    cudaFree(d_cp);
+    if (e2 != cudaSuccess) return fail(SBD_TPB_ERR_CUDA, std::string("occupations: ") + cudaGetErrorString(e2));
+    std::vector<double> occ(2 * (size_t)L, 0.0);
+    auto add = [&](int s, const std::vector<uint64_t> &str, const double *r) {
+      for (size_t i = 0; i < str.size(); i++)
+        for (int p = 0; p < L; p++)
+          if ((str[i] >> p) & 1) occ[2 * p + s] += r[i];
+    };
+    add(0, h->astr, rho.data());
+    add(1, h->bstr, rho.data() + na);
+    std::memcpy(density, occ.data(), sizeof(double) * occ.size());
+    return SBD_TPB_OK;
+  }
+  Rdm R(L);
+  // ---- diagonal part (deterministic: fixed summation order throughout)
   double *d_rho_a = nullptr, *d_rho_b = nullptr, *d_Y = nullptr, *d_Mp = nullptr, *d_cp = nullptr;
   TPB_CUDA(cudaMalloc(&d_rho_a, sizeof(double) * na));
   TPB_CUDA(cudaMalloc(&d_rho_b, sizeof(double) * nb));

@@ -283,7 +283,8 @@ int davidson_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0,
 // <W|H|W> and |HW - E W| (reported unless resid >= 0 is given), then the caller's CI vector,
 // occupations/RDMs and carry-over strings; fills res and returns the solve's status
 int solve_finish(sbd_tpb_handle *h, double *dW, sbd_tpb_result *res,
-                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid);
+                 std::chrono::steady_clock::time_point t0, int nsig, int conv, double resid,
+                 bool sym_w = false);
 // lanczos.cu
 int lanczos_run(sbd_tpb_handle *h, const sbd_tpb_params *p, const double *W0, sbd_tpb_result *res);
 }  // namespace sbdtpb

@@ -971,6 +971,100 @@ __global__ void __launch_bounds__(256)
   block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
 }
 
+// The last step of a Davidson cycle on an exchange-symmetric subspace: W = sum u_k S_k and
+// r = E' W - sum u_k sigma(S_k) from the (bi, bj) tile of each tile pair only (W and r are
+// symmetric), W written to both tiles, W.W and r.r counted twice off the diagonal; no correction.
+// The same W, bit for bit, as residual_kernel (same per-element sums in the same order), from half
+// the subspace bytes.  Each thread streams its chunks of C_k and sigma(S_k) straight into the two
+// sums, so nothing but the sums stays live and the pass runs at full occupancy without staging.
+// partials: [0] W.W, [1] r.r, [2, M + 3) zero (the layout of residual_kernel's).
+template <typename T, int M>
+__global__ void __launch_bounds__(256)
+    residual_w_sym_kernel(ResidualArgs<T> a, uint32_t nb, double *partials) {
+  constexpr int TS = kSymTile, VW = 16 / sizeof(T), TPR = TS / VW, RS = 256 / TPR;
+  __shared__ T Wt[TS][TS + 1];  // W of the (bi, bj) tile, read transposed for (bj, bi)
+  if (a.u_dev) {
+#pragma unroll
+    for (int k = 0; k < M; k++) a.u[k] = __ldg(&a.u_dev[k]);
+    a.e_shifted = __ldg(&a.e_dev[0]);
+  }
+  const uint32_t nt = (nb + TS - 1) / TS;
+  const size_t npairs = (size_t)nt * (nt + 1) / 2;
+  const int cx = (threadIdx.x % TPR) * VW, ty = threadIdx.x / TPR;
+  double acc[M + 3];
+#pragma unroll
+  for (int k = 0; k < M + 3; k++) acc[k] = 0.0;
+  uint32_t bi = 0, bj = 0;
+  if (blockIdx.x < npairs) tile_pair(blockIdx.x, nt, bi, bj);
+  for (size_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const double mult = bi == bj ? 1.0 : 2.0;
+#pragma unroll
+    for (int r = ty; r < TS; r += RS) {
+      const uint32_t i = bi * TS + r, j = bj * TS + cx;
+      if (i >= nb || j >= nb) continue;
+      const size_t base = (size_t)i * nb + j;
+      double w[VW], hc[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) w[l] = hc[l] = 0.0;
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        T c[VW], hv[VW];
+        ldv<T, VW>(a.C.p[k] + base, c);
+        ldv<T, VW>(a.HC.p[k] + base, hv);
+#pragma unroll
+        for (int l = 0; l < VW; l++) {
+          w[l] += a.u[k] * (double)c[l];
+          hc[l] += a.u[k] * (double)hv[l];
+        }
+      }
+      T wv[VW];
+#pragma unroll
+      for (int l = 0; l < VW; l++) {
+        const double rv = a.e_shifted * w[l] - hc[l];
+        acc[0] += mult * w[l] * w[l];
+        acc[1] += mult * rv * rv;
+        wv[l] = (T)w[l];
+        Wt[r][cx + l] = wv[l];
+      }
+      stv<T, VW>(a.W + base, wv);
+    }
+    __syncthreads();
+    if (bi != bj) {
+#pragma unroll
+      for (int r = ty; r < TS; r += RS) {
+        const uint32_t i2 = bj * TS + r, j2 = bi * TS + cx;
+        if (i2 >= nb || j2 >= nb) continue;
+        T v[VW];
+#pragma unroll
+        for (int l = 0; l < VW; l++) v[l] = Wt[cx + l][r];
+        stv<T, VW>(a.W + (size_t)i2 * nb + j2, v);
+      }
+    }
+    __syncthreads();
+    tile_pair_advance(nt, gridDim.x, bi, bj);
+  }
+  block_reduce_store<M + 3>(acc, M + 3, partials, gridDim.x);
+}
+
+// The reference's seeded random start (Randomize, framework/dm_vector.h:101-178): element i is
+// a uniform value in [-1, 1) from a splitmix64-style mix of (seed, i) -- the same integer steps as
+// sbd_elem_hash / sbd_hash_to_uniform (dm_vector.h:100-112), so the same values for any launch
+// shape -- in the reference's determinant order and sign convention; the caller normalises.
+__device__ __forceinline__ double seeded_uniform(unsigned long long seed, unsigned long long i) {
+  unsigned long long x = seed * 6364136223846793005ULL + i * 2862933555777941757ULL;
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ULL;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebULL;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+__global__ void random_start_kernel(double *__restrict__ x, size_t n, unsigned long long seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = seeded_uniform(seed, i);
+}
+
 // Rayleigh-Ritz of the Davidson subspace on one warp.  Hs (ld kMaxSub, column-major, persistent
 // across the steps of a cycle) gets column and row ib = f_k f_ib ov_k; the leading n = ib + 1
 // block is diagonalised by cyclic Jacobi rotations in shared memory (each rotation's row and
@@ -1404,6 +1498,39 @@ int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
   return reduce_into(h, a.m + 3, h->d_scal + slot, grid);
 }
 
+int random_start_vector(sbd_tpb_handle *h, double *x, size_t n, unsigned long long seed) {
+  random_start_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(x, n, seed);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+template <typename T>
+int residual_w_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot) {
+  if (a.m < 1 || a.m > kMaxSub || !a.W || a.t) return fail(SBD_TPB_ERR_INVALID, "residual_w_sym: bad arguments");
+  TPB_CHECK(ensure_scalars(h));
+  const uint32_t nb = (uint32_t)h->bstr.size();
+  const int nblk = h->num_sms * kSymBlocksPerSm;
+  TPB_CHECK(ensure_partials(h, std::max<size_t>((size_t)(kMaxVec + 3) * vec_blocks(h) + kMaxVec + 3,
+                                                (size_t)(kMaxSub + 3) * nblk + 1)));
+  const void *ptrs[2 * kMaxSub + 1];
+  int np = 0;
+  for (int k = 0; k < a.m; k++) {
+    ptrs[np++] = a.C.p[k];
+    ptrs[np++] = a.HC.p[k];
+  }
+  ptrs[np++] = a.W;
+  if (!pair_vec_ok<T>(nb, ptrs, np)) return residual_step_async<T>(h, a, h->ndet(), slot);
+  TPB_CHECK(dispatch_n<1>(a.m, [&](auto K) {
+    constexpr int M = decltype(K)::value;
+    if constexpr (M <= kMaxSub) {
+      residual_w_sym_kernel<T, M><<<nblk, 256, 0, h->stream>>>(a, nb, h->d_partials);
+      TPB_LAUNCHED(h);
+    }
+    return SBD_TPB_OK;
+  }));
+  return reduce_into(h, a.m + 3, h->d_scal + slot, nblk);
+}
+
 template <typename T>
 int cgs_sym_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
                   int want_dots, int slot, int t0_slot, int tt_slot) {
@@ -1474,6 +1601,8 @@ template int symmetrize_dots<double>(sbd_tpb_handle *, double *, const double *c
 template int symmetrize_dots<float>(sbd_tpb_handle *, float *, const float *const *, int, int);
 template int residual_sym_async<double>(sbd_tpb_handle *, const ResidualArgs<double> &, int);
 template int residual_sym_async<float>(sbd_tpb_handle *, const ResidualArgs<float> &, int);
+template int residual_w_sym_async<double>(sbd_tpb_handle *, const ResidualArgs<double> &, int);
+template int residual_w_sym_async<float>(sbd_tpb_handle *, const ResidualArgs<float> &, int);
 template int cgs_sym_async<double>(sbd_tpb_handle *, const double *const *, int, const double *, int, double *, int,
                                    int, int, int);
 template int cgs_sym_async<float>(sbd_tpb_handle *, const float *const *, int, const double *, int, float *, int,

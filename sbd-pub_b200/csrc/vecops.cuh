@@ -56,6 +56,11 @@ int sym_add(sbd_tpb_handle *h, T *x);
 // cgs_second_round_async).
 template <typename T>
 int residual_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot);
+// the reference's seeded random start values (reference order and sign convention, not normalised)
+int random_start_vector(sbd_tpb_handle *h, double *x, size_t n, unsigned long long seed);
+// the last step of a cycle (W out, no correction) on an exchange-symmetric subspace, tile pairs
+template <typename T>
+int residual_w_sym_async(sbd_tpb_handle *h, const ResidualArgs<T> &a, int slot);
 template <typename T>
 int cgs_sym_async(sbd_tpb_handle *h, const T *const *C, int m, const double *coef, int ov_slot, T *t,
                   int want_dots, int slot, int t0_slot = -1, int tt_slot = -1);

@@ -70,7 +70,7 @@ int main(int argc, char **argv) {
     else if (a == "--tolerance") prm.eps = std::atof(next().c_str());
     else if (a == "--max_time") prm.max_time = std::atof(next().c_str());
     else if (a == "--init") prm.init = std::atoi(next().c_str());
-    else if (a == "--seed") next();
+    else if (a == "--seed") prm.seed = std::strtoull(next().c_str(), nullptr, 10);
     else if (a == "--shuffle") do_shuffle = std::atoi(next().c_str());
     else if (a == "--rdm") prm.do_rdm = std::atoi(next().c_str());
     else if (a == "--bit_length") bit_length = std::strtoul(next().c_str(), nullptr, 10);
@@ -105,7 +105,7 @@ int main(int argc, char **argv) {
   if (method != 0 && method != 2) die("only the matrix-free solvers are built: --method 0 (Davidson) or 2 (Lanczos)");
   prm.method = method;
   if (comm_sizes != 1) die("one rank on one GPU: --*_comm_size must be 1");
-  if (prm.init != 0) die("only --init 0 (start from the first determinant) is built");
+  if (prm.init != 0 && prm.init != 1) die("--init must be 0 (first determinant) or 1 (seeded random vector)");
   if (carryover_type < 0 || carryover_type > 3) die("--carryover_type must be 0, 1, 2 or 3");
   if (!unsupported.empty()) die("not built in this version:" + unsupported);
 

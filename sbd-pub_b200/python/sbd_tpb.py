@@ -64,6 +64,7 @@ class Params(C.Structure):
         ("max_it", C.c_int), ("max_nb", C.c_int), ("eps", C.c_double), ("max_time", C.c_double),
         ("init", C.c_int), ("do_rdm", C.c_int), ("precision", C.c_int), ("preconditioner", C.c_int),
         ("verbose", C.c_int), ("device", C.c_int), ("symmetry", C.c_int), ("method", C.c_int),
+        ("seed", C.c_ulonglong),
     ]
 
 

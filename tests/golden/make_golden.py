@@ -57,13 +57,21 @@ CASES = {
     "syn12_co": dict(synthetic=(12, 5, 5, 200, 150, 31), davidson=(10, 10, 1e-10), rdm=False, full=True,
                      carryover=(0.25, 1e-4, 1e-5), lanczos=(3, 30, 1e-10)),
     "fci12": dict(synthetic_named="fci12", davidson=(10, 10, 1e-8), rdm=False, full=False),
+    # init = (init, seed): Davidson from the reference's seeded random start (--init 1 --seed) instead
+    # of the HF determinant; w0 is that start vector as BasisInitVector built it
+    "syn8_init1": dict(synthetic=(8, 3, 3, 56, 56, 11), davidson=(30, 10, 1e-10), rdm=False, full=True,
+                       init=(1, 1729)),
+    "n2_1em3_init1": dict(fcidump=f"{REF}/data/n2/fcidump.txt", adet=f"{REF}/data/n2/1em3-alpha.txt",
+                          davidson=(30, 10, 1e-8), rdm=False, full=False, init=(1, 4242)),
     # the benchmark's larger selected-CI workloads (synthetic_named = a synth.CONFIGS entry): sigma
     # of the closed-form vector (ref_dump --sigma_hash), so a test regenerates its input at any size;
-    # the 16M-determinant set also carries the reference's FP64 Davidson energy.  Only samples and
-    # checksums of the N-vectors are stored.
+    # the 16M- and 100M-determinant sets also carry the reference's FP64 Davidson energy.  Only
+    # samples and checksums of the N-vectors are stored.
     "sci24": dict(synthetic_named="sci24", davidson=(40, 10, 1e-6), rdm=False, full=False, sigma_hash=True,
                   dedupe_tables=True),
     "sci32": dict(synthetic_named="sci32", davidson=None, rdm=False, full=False, sigma_hash=True,
+                  dedupe_tables=True),
+    "sci28": dict(synthetic_named="sci28", davidson=(40, 10, 1e-6), rdm=False, full=False, sigma_hash=True,
                   dedupe_tables=True),
 }
 
@@ -90,6 +98,8 @@ def run_case(name: str, spec: dict, out_dir: str):
         if spec["davidson"]:
             it, nb, tol = spec["davidson"]
             cmd += ["--davidson", str(it), str(nb), repr(tol)]
+        if "init" in spec:
+            cmd += ["--init", str(spec["init"][0]), str(spec["init"][1])]
         if spec["rdm"]:
             cmd += ["--rdm"]
         if "carryover" in spec:
@@ -128,8 +138,10 @@ def run_case(name: str, spec: dict, out_dir: str):
                         ref = ref + 1
                     assert np.array_equal(data.pop(f"{t}_{k}_{part}"), ref), (t, k, part)
             data["tables_deduped"] = np.array([1])
-        for vec in ("hii", "sigma_in", "sigma_out", "W"):
+        for vec in ("hii", "sigma_in", "sigma_out", "W", "w0"):
             if vec == "W" and not spec["davidson"]:
+                continue
+            if vec == "w0" and "init" not in spec:
                 continue
             v = rd(f"{vec}.f64")
             if spec["full"]:
@@ -186,6 +198,8 @@ def run_case(name: str, spec: dict, out_dir: str):
             meta["carryover"] = list(spec["carryover"])
         if "lanczos" in spec:
             meta["lanczos"] = list(spec["lanczos"])
+        if "init" in spec:
+            meta["init"] = list(spec["init"])
         return meta
 
 

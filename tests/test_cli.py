@@ -29,7 +29,7 @@ BAD_FLAGS = [
     (["--bit_length", "65"], "--bit_length must be in [1, 64]"),
     (["--adet_comm_size", "2"], "one rank on one GPU: --*_comm_size must be 1"),
     (["--task_comm_size", "4"], "one rank on one GPU: --*_comm_size must be 1"),
-    (["--init", "1"], "only --init 0"),
+    (["--init", "2"], "--init must be 0 (first determinant) or 1 (seeded random vector)"),
     (["--carryover_type", "4"], "--carryover_type must be 0, 1, 2 or 3"),
     (["--precision", "fp16"], "--precision must be fp64 or mixed"),
     (["--preconditioner", "jacobi"], "--preconditioner must be diagonal or learned"),

@@ -166,6 +166,23 @@ def test_diag_one_shot_rdm_energy(tpb):
     np.testing.assert_allclose(r["density"][0::2] + r["density"][1::2], np.diag(g1), atol=1e-12)
 
 
+@pytest.mark.parametrize("name", ["syn10_ab", "n2_1em3"])
+def test_occupations_alone_equal_rdm_pass(tpb, name):
+    """A solve asked for occupations only (one pass of string weights) reports the same density,
+    bit for bit, as the same solve with the full RDMs, and it matches the reference's 1-RDM
+    diagonal."""
+    h, prob, g, meta = _handle(tpb, name)
+    it, nb, tol = meta["davidson"]
+    p = tpb.default_params(max_it=it, max_nb=nb, eps=tol)
+    a = h.davidson(p, want_vector=False)
+    b = h.davidson(p, want_vector=False, want_rdm=True)
+    assert np.array_equal(a["density"], b["density"])
+    L = prob.norb
+    ref = g["rdm1"]
+    diag = np.concatenate([ref[: L * L].reshape(L, L).diagonal(), ref[L * L:].reshape(L, L).diagonal()])
+    np.testing.assert_allclose(np.concatenate([a["density"][0::2], a["density"][1::2]]), diag, atol=1e-6)
+
+
 def test_invalid_inputs_return_status(tpb):
     prob, g, meta = golden_problem("syn8")
     h = tpb.Handle(0)
