@@ -1,20 +1,22 @@
 """The benchmark's selected-CI workloads pinned to the reference: norb=24 with 4,000 x 4,000 strings
-(16M determinants) and norb=32 with 20,000 x 20,000 strings (400M determinants, the benchmark's
-workload), same seeded generators as bench.py.
+(16M determinants), norb=28 with 10,000 x 10,000 strings (100M, the learned-preconditioner config) and
+norb=32 with 20,000 x 20,000 strings (400M determinants, the benchmark's workload), same seeded
+generators as bench.py.
 
-The fixtures sci24.npz / sci32.npz come from the reference's own code (oracle/_ref/ref_dump, made by
+The fixtures sci24.npz / sci28.npz / sci32.npz come from the reference's own code (oracle/_ref/ref_dump, made by
 tests/golden/make_golden.py): its excitation tables (MakeHelpers + RemakeHelpers, tpb/helper.h:
 710-1226), H_ii (makeQChamDiagTerms, tpb/qcham.h:290-340) and one sigma (mult, tpb/mult.h:625-881) of
 the closed-form vector x_i = ((i * 0x9E3779B97F4A7C15 mod 2^64) >> 11) / 2^53 - 1/2, stored as 512
 sampled entries plus sum / sum of squares / sum of |.| over all N; the 16M set also holds the
 reference's FP64 Davidson energy (tpb/davidson.h:667-930).  The closed form lets every check
-regenerate the input at full size without storing it.
+regenerate the input at full size without storing it.  The 16M and 100M sets also hold the reference's
+FP64 Davidson energy from the HF start.
 
 CPU: the oracle's tables and its sigma at the sampled determinants equal the reference's.
 GPU: the library's tables are bit-exact, H_ii and sigma match at the samples (1e-12 of the largest
 sampled |sigma|) and in the whole-vector sums, sigma matches the oracle at 256 more determinants, and
-at 16M determinants the FP64 Davidson energy is within 1e-8 Ha of the reference's, the mixed one
-within 1e-6 Ha.
+at 16M and 100M determinants the FP64 Davidson energy is within 1e-8 Ha of the reference's, the mixed
+one within 1e-6 Ha.
 """
 import json
 import os
@@ -24,7 +26,7 @@ import pytest
 
 from conftest import GOLDEN, golden_cases
 
-CASES = [c for c in ("sci24", "sci32") if os.path.exists(os.path.join(GOLDEN, f"{c}.npz"))]
+CASES = [c for c in ("sci24", "sci28", "sci32") if os.path.exists(os.path.join(GOLDEN, f"{c}.npz"))]
 K = 0x9E3779B97F4A7C15
 
 
