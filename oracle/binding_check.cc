@@ -8,7 +8,7 @@
 // key=value pairs: the two energies, the largest differences of density, 1-RDM and 2-RDM entries,
 // and whether the carry-over strings are equal (as sets, and in the same order).
 // Usage: binding_check --fcidump F --adetfile A [--iteration I] [--block B] [--tolerance T]
-//                      [--rdm] [--carryover_type K --carryover_threshold X]
+//                      [--rdm] [--carryover_type K --carryover_threshold X] [--init I --seed S]
 //                      [--loadname NAME] [--savename NAME] [--skip_reference]
 #include <chrono>
 #include <cmath>
@@ -54,6 +54,8 @@ int main(int argc, char **argv) {
     else if (a == "--block") s.max_nb = std::atoi(argv[++i]);
     else if (a == "--tolerance") s.eps = std::atof(argv[++i]);
     else if (a == "--rdm") s.do_rdm = 1;
+    else if (a == "--init") s.init = std::atoi(argv[++i]);
+    else if (a == "--seed") s.seed = std::strtoull(argv[++i], nullptr, 10);
     else if (a == "--carryover_type") s.carryover_type = std::atoi(argv[++i]);
     else if (a == "--carryover_threshold") s.threshold = std::atof(argv[++i]);
     else if (a == "--loadname") loadname = argv[++i];

@@ -120,3 +120,16 @@ def test_binding_restart_files(tmp_path):
     out2 = _run([BINDING] + args + ["--loadname", "b_"], tmp_path)
     kv = dict(tok.split("=", 1) for tok in out2.strip().splitlines()[-1].split())
     assert abs(float(kv["e_b200"]) - e1) < 1e-9 and abs(float(kv["e_ref"]) - e1) < 1e-8, kv
+
+
+@needs_ref
+def test_binding_random_start_matches_reference(tmp_path):
+    """--init 1 --seed: the reference's sbd::tpb::diag and the binding start from the same seeded random
+    vector (BasisInitVector with init 1, tpb/davidson.h:138-141) and reach the same energy and RDMs."""
+    prob, meta, base = _inputs(tmp_path)
+    out = _run([BINDING] + base[:4] + ["--iteration", "30", "--block", "10", "--tolerance", "1e-8", "--rdm",
+                                      "--init", "1", "--seed", "4242"], tmp_path)
+    kv = dict(tok.split("=", 1) for tok in out.strip().splitlines()[-1].split())
+    assert abs(float(kv["e_ref"]) - float(kv["e_b200"])) < 1e-8, kv
+    assert abs(float(kv["e_b200"]) - meta["energy"]) < 1e-8, kv
+    assert float(kv["rdm1_diff"]) < 1e-6 and float(kv["rdm2_diff"]) < 1e-6, kv
