@@ -511,46 +511,87 @@ def _solve(h, params, runs=3):
 # random start reaches 2813.1395); the lowest root is exchange-symmetric (unprojected random starts
 # reach it too).
 START = dict(init=1, seed=1729, symmetry=2)
+# seeds of the timed solves: the step count of a solve moves by up to ~20 % with its start and with
+# rounding-level changes, so each arm is timed from several starts and compared by the median
+SEEDS = (1729, 7, 99)
+
+
+def _solve_seeds(h, params_for_seed, e_ref=None):
+    """Per seed the faster of two solves (the solves are deterministic: the same steps, and the
+    faster run drops host-side stalls); the median wall time and steps, every run's time, steps,
+    energy, and (given the lowest-root energy) whether it reached that state, with the median time
+    of the runs that did."""
+    import statistics as st
+
+    def one(seed):
+        r = _solve(h, params_for_seed(seed), runs=2)
+        r["seconds"] = min(r["seconds_runs"])
+        r["ms_per_step"] = 1e3 * r["seconds"] / max(1, r["sigma_steps"])
+        return r
+    runs = [(s, one(s)) for s in SEEDS]
+    out = {"seconds": st.median(r["seconds"] for _, r in runs),
+           "sigma_steps": st.median(r["sigma_steps"] for _, r in runs),
+           "ms_per_step": st.median(r["ms_per_step"] for _, r in runs),
+           "seeds": list(SEEDS), "seconds_runs": [r["seconds"] for _, r in runs],
+           "sigma_steps_runs": [r["sigma_steps"] for _, r in runs],
+           "energy_runs": [r["energy"] for _, r in runs], "residual_runs": [r["residual"] for _, r in runs],
+           "converged_runs": [r["converged"] for _, r in runs],
+           "learned_steps_runs": [r["learned_steps"] for _, r in runs],
+           "fallback_steps_runs": [r["fallback_steps"] for _, r in runs], "eps": runs[0][1]["eps"]}
+    if e_ref is not None:
+        out["abs_energy_error_runs"] = [abs(e - e_ref) for e in out["energy_runs"]]
+        out["on_lowest_root_runs"] = [d < 1e-6 for d in out["abs_energy_error_runs"]]
+        ok = [t for t, on in zip(out["seconds_runs"], out["on_lowest_root_runs"]) if on]
+        out["reached_lowest_root"] = f"{len(ok)}/{len(SEEDS)}"
+        out["seconds_on_lowest_root"] = st.median(ok) if ok else None
+    return out
 
 
 def time_to_solution(h, args, pc):
-    """Wall time of whole Davidson solves for the lowest root: the FP64 reference answer (residual
-    1e-6), then plain FP64, mixed precision and mixed precision + learned preconditioner, all to
-    residual 1e-4 (energy error ~ residual^2 when a solve lands on the same state), median of three
-    solves each, all from the seeded random start (START).  A solve that stops on another state
-    shows it in abs_energy_error_vs_fp64_reference (the residual test cannot tell the states
-    apart).  The HF-started solves (the reference app's default start) are timed once each beside
-    them, with the state they reach."""
+    """Wall time of whole Davidson solves for the lowest root, each arm from the seeded random
+    starts of SEEDS (projected onto the exchange-symmetric sector): the FP64 reference solves
+    (residual 1e-6; the lowest of their energies is the lowest root), then plain FP64, mixed
+    precision and mixed precision + learned preconditioner to residual 1e-4 (energy error ~
+    residual^2 on the same state).  Per arm the median over the seeds; every run's steps, energy and
+    whether it reached the lowest root (the residual test cannot tell the states apart, and a
+    single-vector restart can settle on an excited state).  The HF-started solves (the reference
+    app's default start) are timed once each beside them, with the state they reach."""
     import sbd_tpb
     out = {}
-    par = lambda **kw: sbd_tpb.default_params(max_it=60, max_nb=8, **START, **kw)  # noqa: E731
-    out["fp64_reference"] = _solve(h, par(eps=1e-6, precision=sbd_tpb.FP64), runs=1)
-    out["fp64"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.FP64))
-    out["mixed"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.MIXED))
+    base = dict(max_it=60, max_nb=8, init=1, symmetry=2)
+    par = lambda eps, **kw: (lambda seed: sbd_tpb.default_params(eps=eps, seed=seed, **base, **kw))  # noqa: E731
+    ref = _solve_seeds(h, par(1e-6, precision=sbd_tpb.FP64))
+    e_ref = min(ref["energy_runs"])
+    ref["abs_energy_error_runs"] = [abs(e - e_ref) for e in ref["energy_runs"]]
+    out["fp64_reference"] = ref
+    out["lowest_root"] = e_ref
+    out["fp64"] = _solve_seeds(h, par(1e-4, precision=sbd_tpb.FP64), e_ref)
+    out["mixed"] = _solve_seeds(h, par(1e-4, precision=sbd_tpb.MIXED), e_ref)
     h.set_preconditioner(pc)
-    out["mixed_learned"] = _solve(h, par(eps=1e-4, precision=sbd_tpb.MIXED,
-                                         preconditioner=sbd_tpb.PRECOND_LEARNED))
+    out["mixed_learned"] = _solve_seeds(h, par(1e-4, precision=sbd_tpb.MIXED,
+                                               preconditioner=sbd_tpb.PRECOND_LEARNED), e_ref)
     h.set_preconditioner(None)
-    e_ref = out["fp64_reference"]["energy"]
-    for k in ("fp64", "mixed", "mixed_learned"):
-        out[k]["abs_energy_error_vs_fp64_reference"] = abs(out[k]["energy"] - e_ref)
-        out[k]["same_state_as_reference"] = out[k]["abs_energy_error_vs_fp64_reference"] < 1e-6
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["speedup_mixed_learned_vs_fp64"] = out["fp64"]["seconds"] / out["mixed_learned"]["seconds"]
-    # per Davidson step (what the precision changes; the step counts move with last-bit rounding)
+    # the same from the medians of the runs that reached the lowest root (a run that stops on an
+    # excited state has not solved the problem)
+    on = {k: out[k]["seconds_on_lowest_root"] for k in ("fp64", "mixed", "mixed_learned")}
+    out["speedup_mixed_vs_fp64_on_lowest_root"] = on["fp64"] / on["mixed"] if on["fp64"] and on["mixed"] else None
+    out["speedup_mixed_learned_vs_fp64_on_lowest_root"] = (on["fp64"] / on["mixed_learned"]
+                                                           if on["fp64"] and on["mixed_learned"] else None)
+    # per Davidson step (what the precision changes)
     out["per_step_speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
-    out["start"] = ("seeded random vector (--init 1 --seed 1729, the reference's Randomize) projected onto "
-                    "the exchange-symmetric sector")
+    out["start"] = ("seeded random vectors (--init 1 --seed S, the reference's Randomize; S in seeds) projected "
+                    "onto the exchange-symmetric sector")
     hf = lambda **kw: sbd_tpb.default_params(max_it=40, max_nb=8, eps=1e-4, **kw)  # noqa: E731
     out["hf_start"] = {"fp64": _solve(h, hf(precision=sbd_tpb.FP64), runs=1),
                        "mixed": _solve(h, hf(precision=sbd_tpb.MIXED), runs=1)}
     for v in out["hf_start"].values():
         v["energy_above_lowest_root"] = v["energy"] - e_ref
     out["note"] = ("training (pairs from the 12- and 24-orbital problems) is timed separately and not "
-                   "part of the solve times; seconds = the median of seconds_runs (three runs of each "
-                   "compared solve); the solves are deterministic, so the three runs take the same steps; "
-                   "hf_start: the same solvers from the HF determinant (--init 0), which converge to an "
-                   "excited state on this Hamiltonian")
+                   "part of the solve times; seconds = the median over the seeds of the faster of two solves "
+                   "each (the solves are deterministic); hf_start: the same solvers from the HF determinant "
+                   "(--init 0), which converge to an excited state on this Hamiltonian")
     return out
 
 
