@@ -479,6 +479,322 @@ __global__ void reorder_sign_kernel_f32(const uint64_t *__restrict__ apar,
   }
 }
 
+// The general alpha and beta passes with CM column groups per thread, as sigma_sym_cm_kernel does
+// for the one-pass form: each thread covers CM 16-byte column groups TC * VW columns apart and reuses
+// each staged table entry for all of them.  16-byte rows and no alpha-single x beta-single terms
+// (the caller falls back to sigma_block_kernel otherwise).  The alpha pass (X = C) adds the diagonal,
+// writes sigma once and its own C values transposed into C^T (parked in shared memory when OS); the
+// beta pass (X = C^T) adds its sums into sigma transposed.  Same per-element arithmetic and order
+// as sigma_block_kernel, so the same bits.
+template <typename T, bool kAlpha, int G, int M, int CM, bool OS>
+__global__ void __launch_bounds__(kBlkThreads, M)
+    sigma_pass_cm_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out, T *__restrict__ XT) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int TC = kBlkThreads / G;
+  constexpr int RPT = kBlkRows / G;
+  constexpr int W = CM * TC * VW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *sd_ket = reinterpret_cast<uint32_t *>(smem_raw);
+  T *sd_val = reinterpret_cast<T *>(smem_raw + ((a.max_d * 4 + 15) & ~15u));
+  unsigned char *sp = smem_raw + ((a.max_d * 4 + 15) & ~15u) + a.max_d * sizeof(T);
+  sp = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sp) + 15) & ~(uintptr_t)15);
+  uint32_t *ss_ket = reinterpret_cast<uint32_t *>(sp);
+  int32_t *ss_pair = reinterpret_cast<int32_t *>(sp + a.max_s * 4);
+  double *ss_val = reinterpret_cast<double *>(sp + ((a.max_s * 8 + 15) & ~15u));
+  // OS: [row][column group][element][thread], conflict-free
+  T *own_s = reinterpret_cast<T *>((reinterpret_cast<uintptr_t>(ss_val + a.max_s) + 15) & ~(uintptr_t)15);
+
+  const uint32_t nrb = (a.nrows + kBlkRows - 1) / kBlkRows;
+  const uint32_t rb = blockIdx.x % nrb, slab = blockIdx.x / nrb;
+  const uint32_t r0 = rb * kBlkRows;
+  const uint32_t ncols = a.ncols;
+  const int nr = (int)min((uint32_t)kBlkRows, a.nrows - r0);
+  const int grp = threadIdx.x / TC;
+  uint32_t cb[CM];
+  bool full[CM];
+#pragma unroll
+  for (int g = 0; g < CM; g++) {
+    cb[g] = slab * W + g * TC * VW + (threadIdx.x % TC) * VW;
+    full[g] = cb[g] + VW <= ncols;  // ncols is a multiple of VW: a group is all in or all out
+  }
+
+  const uint32_t dlo = __ldg(&a.d_off[r0]), dhi = __ldg(&a.d_off[r0 + nr]);
+  const uint32_t slo = __ldg(&a.s_off[r0]), shi = __ldg(&a.s_off[r0 + nr]);
+  for (uint32_t e = dlo + threadIdx.x; e < dhi; e += blockDim.x) {
+    sd_ket[e - dlo] = __ldg(&a.d_ket[e]);
+    sd_val[e - dlo] = val_of<T>(a.d_val, a.d_valf, e);
+  }
+  for (uint32_t e = slo + threadIdx.x; e < shi; e += blockDim.x) {
+    ss_ket[e - slo] = __ldg(&a.s_ket[e]);
+    ss_pair[e - slo] = __ldg(&a.s_pair[e]);
+    ss_val[e - slo] = (double)val_of<T>(a.s_val, a.s_valf, e);
+  }
+  __syncthreads();
+  if (!full[0]) return;
+
+  T acc[RPT][CM][VW];
+  T own[(kAlpha && !OS) ? RPT : 1][CM][VW];
+#pragma unroll
+  for (int r = 0; r < RPT; r++)
+#pragma unroll
+    for (int g = 0; g < CM; g++)
+#pragma unroll
+      for (int i = 0; i < VW; i++) {
+        acc[r][g][i] = T(0);
+        if (kAlpha && !OS) own[r][g][i] = T(0);
+      }
+  const int rlo = grp * RPT;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    if (rlo + r >= nr) continue;
+    const uint32_t row = r0 + rlo + r;
+    const uint32_t d0 = __ldg(&a.d_off[row]) - dlo, d1 = __ldg(&a.d_off[row + 1]) - dlo;
+#pragma unroll 4
+    for (uint32_t e = d0; e < d1; e++) {
+      const T v = sd_val[e];
+      const T *xr = X + (size_t)sd_ket[e] * ncols;
+#pragma unroll
+      for (int g = 0; g < CM; g++) {
+        if (g > 0 && !full[g]) continue;
+        Vec<T, VW, true> x;
+        x.load(xr + cb[g]);
+#pragma unroll
+        for (int i = 0; i < VW; i++) acc[r][g][i] += v * x.v[i];
+      }
+    }
+    const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
+    for (uint32_t e = s0; e < s1; e++) {
+      const uint32_t ket = ss_ket[e];
+      const double v = ss_val[e];
+      const int32_t ps = ss_pair[e];
+      const int pr = (ps > 0 ? ps : -ps) - 1;
+      const double sg = ps > 0 ? 1.0 : -1.0;
+      const double *vrow = a.vd + (size_t)pr * a.L;
+      const T *xr = X + (size_t)ket * ncols;
+      const double *jr = a.jtab ? a.jtab + (size_t)__ldg(&a.pmap[pr]) * ncols : nullptr;
+#pragma unroll
+      for (int g = 0; g < CM; g++) {
+        if (g > 0 && !full[g]) continue;
+        Vec<T, VW, true> xv;
+        xv.load(xr + cb[g]);
+        double o[VW];
+        if (jr) {
+#pragma unroll
+          for (int i = 0; i < VW; i += 2) {
+            const double2 jj = __ldg(reinterpret_cast<const double2 *>(jr + cb[g] + i));
+            o[i] = jj.x;
+            o[i + 1] = jj.y;
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < VW; i++) {
+            uint64_t occ = __ldg(&a.col_str[cb[g] + i]);
+            o[i] = 0.0;
+            while (occ) {
+              o[i] += __ldg(&vrow[lowest_bit(occ)]);
+              occ &= occ - 1;
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+      }
+    }
+    if constexpr (kAlpha) {
+      const T *hsrc = sizeof(T) == 8 ? reinterpret_cast<const T *>(a.hii) : reinterpret_cast<const T *>(a.hii32);
+      const double hshift = sizeof(T) == 8 ? -a.core_shift : a.core_shift;
+#pragma unroll
+      for (int g = 0; g < CM; g++) {
+        if (g > 0 && !full[g]) continue;
+        const size_t idx = (size_t)row * ncols + cb[g];
+        Vec<T, VW, true> xo, hv, ov;
+        xo.load(X + idx);
+        hv.load(hsrc + idx);
+        if (a.accumulate) ov.load_rw(out + idx);
+#pragma unroll
+        for (int i = 0; i < VW; i++) {
+          if (OS) own_s[((r * CM + g) * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
+          else own[OS ? 0 : r][g][i] = xo.v[i];
+          double res = (double)acc[r][g][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+          if (a.accumulate) res += (double)ov.v[i];
+          ov.v[i] = (T)res;
+        }
+        ov.store(out + idx);
+      }
+    }
+  }
+  // transposed write-out: column c gets this thread's rows contiguous (index c * nrows + r), as
+  // 16-byte accesses when the block is full and the thread's rows form whole 16-byte runs
+  constexpr int RW = 16 / sizeof(T);
+  constexpr bool kRuns = RPT % RW == 0;
+  const bool vec_out = kRuns && nr == kBlkRows && (a.nrows % RW) == 0;
+#pragma unroll
+  for (int g = 0; g < CM; g++) {
+    if (g > 0 && !full[g]) continue;
+#pragma unroll
+    for (int i = 0; i < VW; i++) {
+      const size_t o = (size_t)(cb[g] + i) * a.nrows + r0 + rlo;
+      if constexpr (kRuns) {
+        if (vec_out) {
+#pragma unroll
+          for (int r = 0; r < RPT; r += RW) {
+            Vec<T, RW, true> v;
+            if (kAlpha) {
+#pragma unroll
+              for (int q = 0; q < RW; q++)
+                v.v[q] = OS ? own_s[(((r + q) * CM + g) * VW + i) * kBlkThreads + threadIdx.x]
+                            : own[OS ? 0 : r + q][g][i];
+            } else {
+              v.load_rw(out + o + r);
+#pragma unroll
+              for (int q = 0; q < RW; q++) v.v[q] += acc[r + q][g][i];
+            }
+            v.store(kAlpha ? XT + o + r : out + o + r);
+          }
+          continue;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RPT; r++) {
+        if (rlo + r < nr) {
+          if (kAlpha) XT[o + r] = OS ? own_s[((r * CM + g) * VW + i) * kBlkThreads + threadIdx.x] : own[OS ? 0 : r][g][i];
+          else out[o + r] += acc[r][g][i];
+        }
+      }
+    }
+  }
+}
+
+// The one-pass symmetric alpha pass with CM column groups per thread: each thread covers CM
+// 16-byte groups of columns, TC * VW columns apart (so every load of a warp is one contiguous
+// 512-byte run), and reuses each staged table entry -- its ket, value, and address arithmetic -- for
+// all CM groups.  16-byte rows only (the caller falls back to sigma_block_kernel otherwise).  Same
+// per-element arithmetic and order as sigma_block_kernel<kSym>.
+template <typename T, int G, int M, int CM>
+__global__ void __launch_bounds__(kBlkThreads, M)
+    sigma_sym_cm_kernel(BlockArgs a, const T *__restrict__ X, T *__restrict__ out) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int TC = kBlkThreads / G;
+  constexpr int RPT = kBlkRows / G;
+  constexpr int W = CM * TC * VW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *sd_ket = reinterpret_cast<uint32_t *>(smem_raw);
+  T *sd_val = reinterpret_cast<T *>(smem_raw + ((a.max_d * 4 + 15) & ~15u));
+  unsigned char *sp = smem_raw + ((a.max_d * 4 + 15) & ~15u) + a.max_d * sizeof(T);
+  sp = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sp) + 15) & ~(uintptr_t)15);
+  uint32_t *ss_ket = reinterpret_cast<uint32_t *>(sp);
+  int32_t *ss_pair = reinterpret_cast<int32_t *>(sp + a.max_s * 4);
+  double *ss_val = reinterpret_cast<double *>(sp + ((a.max_s * 8 + 15) & ~15u));
+
+  const uint32_t nrb = (a.nrows + kBlkRows - 1) / kBlkRows;
+  const uint32_t rb = blockIdx.x % nrb, slab = blockIdx.x / nrb;
+  const uint32_t r0 = rb * kBlkRows;
+  const uint32_t ncols = a.ncols;
+  const int nr = (int)min((uint32_t)kBlkRows, a.nrows - r0);
+  const int grp = threadIdx.x / TC;
+  uint32_t cb[CM];
+  bool full[CM];
+#pragma unroll
+  for (int g = 0; g < CM; g++) {
+    cb[g] = slab * W + g * TC * VW + (threadIdx.x % TC) * VW;
+    full[g] = cb[g] + VW <= ncols;  // ncols is a multiple of VW: a group is all in or all out
+  }
+
+  const uint32_t dlo = __ldg(&a.d_off[r0]), dhi = __ldg(&a.d_off[r0 + nr]);
+  const uint32_t slo = __ldg(&a.s_off[r0]), shi = __ldg(&a.s_off[r0 + nr]);
+  for (uint32_t e = dlo + threadIdx.x; e < dhi; e += blockDim.x) {
+    sd_ket[e - dlo] = __ldg(&a.d_ket[e]);
+    sd_val[e - dlo] = val_of<T>(a.d_val, a.d_valf, e);
+  }
+  for (uint32_t e = slo + threadIdx.x; e < shi; e += blockDim.x) {
+    ss_ket[e - slo] = __ldg(&a.s_ket[e]);
+    ss_pair[e - slo] = __ldg(&a.s_pair[e]);
+    ss_val[e - slo] = (double)val_of<T>(a.s_val, a.s_valf, e);
+  }
+  __syncthreads();
+  if (!full[0]) return;
+
+  T acc[RPT][CM][VW];
+#pragma unroll
+  for (int r = 0; r < RPT; r++)
+#pragma unroll
+    for (int g = 0; g < CM; g++)
+#pragma unroll
+      for (int i = 0; i < VW; i++) acc[r][g][i] = T(0);
+  const int rlo = grp * RPT;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    if (rlo + r >= nr) continue;
+    const uint32_t row = r0 + rlo + r;
+    const uint32_t d0 = __ldg(&a.d_off[row]) - dlo, d1 = __ldg(&a.d_off[row + 1]) - dlo;
+#pragma unroll 4
+    for (uint32_t e = d0; e < d1; e++) {
+      const T v = sd_val[e];
+      const T *xr = X + (size_t)sd_ket[e] * ncols;
+#pragma unroll
+      for (int g = 0; g < CM; g++) {
+        if (g > 0 && !full[g]) continue;
+        Vec<T, VW, true> x;
+        x.load(xr + cb[g]);
+#pragma unroll
+        for (int i = 0; i < VW; i++) acc[r][g][i] += v * x.v[i];
+      }
+    }
+    const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
+    for (uint32_t e = s0; e < s1; e++) {
+      const uint32_t ket = ss_ket[e];
+      const double v = ss_val[e];
+      const int32_t ps = ss_pair[e];
+      const int pr = (ps > 0 ? ps : -ps) - 1;
+      const double sg = ps > 0 ? 1.0 : -1.0;
+      const double *vrow = a.vd + (size_t)pr * a.L;
+      const T *xr = X + (size_t)ket * ncols;
+      const double *jr = a.jtab ? a.jtab + (size_t)__ldg(&a.pmap[pr]) * ncols : nullptr;
+#pragma unroll
+      for (int g = 0; g < CM; g++) {
+        if (g > 0 && !full[g]) continue;
+        Vec<T, VW, true> xv;
+        xv.load(xr + cb[g]);
+        double o[VW];
+        if (jr) {
+#pragma unroll
+          for (int i = 0; i < VW; i += 2) {
+            const double2 jj = __ldg(reinterpret_cast<const double2 *>(jr + cb[g] + i));
+            o[i] = jj.x;
+            o[i + 1] = jj.y;
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < VW; i++) {
+            uint64_t occ = __ldg(&a.col_str[cb[g] + i]);
+            o[i] = 0.0;
+            while (occ) {
+              o[i] += __ldg(&vrow[lowest_bit(occ)]);
+              occ &= occ - 1;
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+      }
+    }
+    const T *hsrc = sizeof(T) == 8 ? reinterpret_cast<const T *>(a.hii) : reinterpret_cast<const T *>(a.hii32);
+    const double hshift = sizeof(T) == 8 ? -a.core_shift : a.core_shift;
+#pragma unroll
+    for (int g = 0; g < CM; g++) {
+      if (g > 0 && !full[g]) continue;
+      const size_t idx = (size_t)row * ncols + cb[g];
+      Vec<T, VW, true> xo, hv, ov;
+      xo.load(X + idx);
+      hv.load(hsrc + idx);
+#pragma unroll
+      for (int i = 0; i < VW; i++)
+        ov.v[i] = (T)((double)acc[r][g][i] + 0.5 * (((double)hv.v[i] + hshift) * (double)xo.v[i]));
+      ov.store(out + idx);
+    }
+  }
+}
+
 }  // namespace
 
 int reorder_sign_apply_f64(sbd_tpb_handle *h, const double *x, double *y) {
@@ -518,6 +834,25 @@ int launch_block_cfg(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out,
   return SBD_TPB_OK;
 }
 
+// sigma_pass_cm_kernel launch (16-byte rows, no alpha-single x beta-single terms)
+template <typename T, bool kAlpha, int G, int M, int CM, bool OS = false>
+int launch_pass_cm(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int W = CM * (kBlkThreads / G) * VW;
+  const size_t nrb = (ba.nrows + kBlkRows - 1) / kBlkRows, nslab = (ba.ncols + W - 1) / W;
+  const size_t blocks = nrb * nslab;
+  if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
+  const size_t smem = ((ba.max_d * 4 + 15) & ~(size_t)15) + (size_t)ba.max_d * sizeof(T) + 16 +
+                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16 +
+                      (OS ? (size_t)(kBlkRows / G) * CM * VW * kBlkThreads * sizeof(T) + 16 : 0);
+  if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
+  auto kern = sigma_pass_cm_kernel<T, kAlpha, G, M, CM, OS>;
+  TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out, XT);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
 template <typename T, bool kAlpha>
 int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
   if constexpr (sizeof(T) == 4 && kAlpha) {
@@ -534,14 +869,40 @@ int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *
   }
 }
 
-// The symmetric alpha pass: no C^T and no values kept for it.  Launch shapes from a sweep (CUDA
-// events, ms at 4e8 / 1e8 determinants): FP32 2 row groups at 8 CTAs/SM 2.78 / 1.23 (a 148-byte
-// spill; 2/7 2.96 / 1.29, 4/8 3.02 / 1.30, 1/6 3.11 / 1.33, 2/6 3.32 / 1.40), FP64 2/8 4.83 / 2.08
-// (2/9 with a 192-byte spill 4.61 / 2.19, 2/7 5.18 / 2.18, 4/8 5.49 / 2.31, 1/4 6.43 / 2.68).
+// sigma_sym_cm_kernel launch (16-byte rows only)
+template <typename T, int G, int M, int CM>
+int launch_sym_cm(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int W = CM * (kBlkThreads / G) * VW;
+  if ((ba.ncols % VW) || (reinterpret_cast<uintptr_t>(X) % 16) || (reinterpret_cast<uintptr_t>(out) % 16))
+    return fail(SBD_TPB_ERR_INVALID, "sigma: one-pass kernel needs 16-byte rows");
+  const size_t nrb = (ba.nrows + kBlkRows - 1) / kBlkRows, nslab = (ba.ncols + W - 1) / W;
+  const size_t blocks = nrb * nslab;
+  if (blocks > 0x7fffffffull) return fail(SBD_TPB_ERR_INVALID, "sigma: grid too large");
+  const size_t smem = ((ba.max_d * 4 + 15) & ~(size_t)15) + (size_t)ba.max_d * sizeof(T) + 16 +
+                      ((ba.max_s * 8 + 15) & ~(size_t)15) + (size_t)ba.max_s * 8 + 16;
+  if (smem > h->smem_optin) return fail(SBD_TPB_ERR_INVALID, "sigma: table block exceeds shared memory");
+  auto kern = sigma_sym_cm_kernel<T, G, M, CM>;
+  TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)blocks, kBlkThreads, smem, h->stream>>>(ba, X, out);
+  TPB_LAUNCHED(h);
+  return SBD_TPB_OK;
+}
+
+// The symmetric alpha pass: no C^T and no values kept for it.  Launch shapes from sweeps (CUDA
+// events, ms at 4e8 / 1e8 determinants), all giving the same bits.  With two column groups per
+// thread (sigma_sym_cm_kernel, row groups / CTAs per SM / column groups): FP32 4/10/2 2.03 / 0.95,
+// 2/8/2 2.09 / 0.99, 2/6/2 2.10 / 0.99, 4/8/2 2.14 / 0.97, 4/12/2 2.07 / 1.31, and one column
+// group 2/8/1 2.19 / 1.01; FP64 2/8/2 3.77 / 1.75, 4/10/2 3.81 / 2.08, 2/6/2 4.04 / 1.82, 4/8/2
+// 4.17 / 1.82, 2/8/1 4.17 / 2.13.  The general kernel's form (sigma_block_kernel<kSym>, kept for
+// rows that are not 16-byte aligned) took FP32 2.78 / 1.22 and FP64 4.83 / 2.08 at its best shape.
 template <typename T>
 int launch_block_sym(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out) {
-  if constexpr (sizeof(T) == 4) return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
-  else return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
+  const bool rows16 = (ba.ncols % (16 / sizeof(T))) == 0 && reinterpret_cast<uintptr_t>(X) % 16 == 0 &&
+                      reinterpret_cast<uintptr_t>(out) % 16 == 0;
+  if (!rows16) return launch_block_cfg<T, true, 2, 8, false, true>(h, ba, X, out, nullptr);
+  if constexpr (sizeof(T) == 4) return launch_sym_cm<T, 4, 10, 2>(h, ba, X, out);
+  else return launch_sym_cm<T, 2, 8, 2>(h, ba, X, out);
 }
 
 // Most entries of any kBlkRows-row block of a CSR table of n rows (shared-memory staging size).
