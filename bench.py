@@ -44,11 +44,13 @@ sys.path.insert(0, os.path.join(ROOT, "sbd-pub_b200", "python"))
 
 METRIC = "sigma GDets/s; time to 1e-6 Ha: mixed+learned vs plain FP64, 1 B200"
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
-# DRAM bytes (read + write) per determinant of one launch of the FP64 sigma passes, from an ncu
-# capture of both kernels at 10^8 determinants (norb=28, 10,000 x 10,000 strings): alpha
-# 1.781 + 1.566 GB, beta 1.719 + 0.765 GB
-TRAFFIC_F64_ALPHA = 33.47
-TRAFFIC_F64_BETA = 24.84
+# DRAM bytes (read + write) per determinant of one launch of each sigma pass, from an ncu capture
+# of the passes at 10^8 determinants (norb=28, 10,000 x 10,000 strings): FP64 alpha 2.232 + 1.569 GB,
+# beta 2.019 + 0.768 GB; FP32 alpha 1.205 + 0.836 GB, beta 1.251 + 0.410 GB
+TRAFFIC_F64_ALPHA = 38.01
+TRAFFIC_F64_BETA = 27.87
+TRAFFIC_F32_ALPHA = 20.42
+TRAFFIC_F32_BETA = 16.61
 
 
 def parse():
@@ -661,7 +663,7 @@ def kernel_breakdown(h, prob, x, y, esz, reps):
     def table_bytes(singles, doubles):
         ns, nd = int(h.table(singles)[1].size), int(h.table(doubles)[1].size)
         return ns * (4 + esz + 4) + nd * (4 + esz) + 8 * (len(prob.astr) + 1)
-    names = ["sigma_block_kernel<alpha>", "sigma_block_kernel<beta>", "alpha_beta_term"][:len(kern)]
+    names = ["sigma_pass_cm_kernel<alpha>", "sigma_pass_cm_kernel<beta>", "alpha_beta_term"][:len(kern)]
     per = [3 * N * esz + N * esz + table_bytes(0, 1), 3 * N * esz + table_bytes(2, 3),
            2 * N * esz + table_bytes(0, 2) // 4][:len(kern)]
     return names, kern, per
@@ -709,9 +711,10 @@ def run_ours(args, world, rank, local, pg):
     # DRAM bytes per determinant of the dominant pass, from one ncu capture of that kernel at
     # 10^8 determinants (norb=28), scaled by determinants: DRAM traffic of these passes grows in
     # proportion to the vectors they stream
-    traffic_per_det = {(8, "sigma_block_kernel<alpha>"): TRAFFIC_F64_ALPHA,
-                       (8, "sigma_block_kernel<beta>"): TRAFFIC_F64_BETA,
-                       (4, "sigma_block_kernel<alpha>"): 17.69, (4, "sigma_block_kernel<beta>"): 12.60}
+    traffic_per_det = {(8, "sigma_pass_cm_kernel<alpha>"): TRAFFIC_F64_ALPHA,
+                       (8, "sigma_pass_cm_kernel<beta>"): TRAFFIC_F64_BETA,
+                       (4, "sigma_pass_cm_kernel<alpha>"): TRAFFIC_F32_ALPHA,
+                       (4, "sigma_pass_cm_kernel<beta>"): TRAFFIC_F32_BETA}
     tpd = traffic_per_det.get((esz, names[dom]))
     traffic = tpd * N / 1e9 if tpd else None
     roofline = {"kernel": names[dom], "bound": "hbm", "achieved": achieved,

@@ -50,6 +50,12 @@ __device__ __forceinline__ float val_of<float>(const double *, const float *vf, 
   return __ldg(&vf[e]);
 }
 
+// The element arithmetic of every sigma pass, written out so that each kernel form rounds the same
+// way (no contraction left to the compiler): doubles term acc + v x as one fused multiply-add, the
+// singles term and the diagonal as a rounded FP64 product added to the accumulator.
+__device__ __forceinline__ float madd(float acc, float v, float x) { return __fmaf_rn(v, x, acc); }
+__device__ __forceinline__ double madd(double acc, double v, double x) { return __fma_rn(v, x, acc); }
+
 // VW consecutive elements of type T: one 16-byte load when kVec, VW scalars otherwise.
 template <typename T, int VW, bool kVec>
 struct Vec;
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
         for (int i = 0; i < VW; i++) x.v[i] = ok[i] ? __ldg(xr + i) : T(0);
       }
 #pragma unroll
-      for (int i = 0; i < VW; i++) acc[r][i] += v * x.v[i];
+      for (int i = 0; i < VW; i++) acc[r][i] = madd(acc[r][i], v, x.v[i]);
     }
     const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
     for (uint32_t e = s0; e < s1; e++) {
@@ -248,7 +254,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
           o[i + 1] = jj.y;
         }
 #pragma unroll
-        for (int i = 0; i < VW; i++) acc[r][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+        for (int i = 0; i < VW; i++) acc[r][i] += (T)__dmul_rn(v + sg * o[i], (double)xv.v[i]);
         continue;
       }
 #pragma unroll
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
             occ &= occ - 1;
           }
         }
-        double x = (v + sg * o) * (double)__ldg(&xr[c]);
+        double x = __dmul_rn(v + sg * o, (double)__ldg(&xr[c]));
         if (kAlpha && a.do_ab) {
           // this alpha single (ket = Ja, pair pr, sign sg) x every beta single of column Ib
           const uint32_t f1 = __ldg(&a.bs_off[c + 1]);
@@ -303,11 +309,11 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       for (int i = 0; i < VW; i++) {
         double res;
         if constexpr (kSym) {
-          res = (double)acc[r][i] + 0.5 * (((double)hv.v[i] + hshift) * (double)xo.v[i]);
+          res = (double)acc[r][i] + 0.5 * __dmul_rn((double)hv.v[i] + hshift, (double)xo.v[i]);
         } else {
           if (OS) own_s[(r * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
           else own[r][i] = xo.v[i];
-          res = (double)acc[r][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+          res = (double)acc[r][i] + __dmul_rn((double)hv.v[i] + hshift, (double)xo.v[i]);
         }
         if (a.accumulate) res += (double)ov.v[i];
         ov.v[i] = (T)res;
@@ -559,7 +565,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
         Vec<T, VW, true> x;
         x.load(xr + cb[g]);
 #pragma unroll
-        for (int i = 0; i < VW; i++) acc[r][g][i] += v * x.v[i];
+        for (int i = 0; i < VW; i++) acc[r][g][i] = madd(acc[r][g][i], v, x.v[i]);
       }
     }
     const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
@@ -597,7 +603,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
           }
         }
 #pragma unroll
-        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)__dmul_rn(v + sg * o[i], (double)xv.v[i]);
       }
     }
     if constexpr (kAlpha) {
@@ -615,7 +621,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
         for (int i = 0; i < VW; i++) {
           if (OS) own_s[((r * CM + g) * VW + i) * kBlkThreads + threadIdx.x] = xo.v[i];
           else own[OS ? 0 : r][g][i] = xo.v[i];
-          double res = (double)acc[r][g][i] + ((double)hv.v[i] + hshift) * (double)xo.v[i];
+          double res = (double)acc[r][g][i] + __dmul_rn((double)hv.v[i] + hshift, (double)xo.v[i]);
           if (a.accumulate) res += (double)ov.v[i];
           ov.v[i] = (T)res;
         }
@@ -737,7 +743,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
         Vec<T, VW, true> x;
         x.load(xr + cb[g]);
 #pragma unroll
-        for (int i = 0; i < VW; i++) acc[r][g][i] += v * x.v[i];
+        for (int i = 0; i < VW; i++) acc[r][g][i] = madd(acc[r][g][i], v, x.v[i]);
       }
     }
     const uint32_t s0 = __ldg(&a.s_off[row]) - slo, s1 = __ldg(&a.s_off[row + 1]) - slo;
@@ -775,7 +781,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
           }
         }
 #pragma unroll
-        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)((v + sg * o[i]) * (double)xv.v[i]);
+        for (int i = 0; i < VW; i++) acc[r][g][i] += (T)__dmul_rn(v + sg * o[i], (double)xv.v[i]);
       }
     }
     const T *hsrc = sizeof(T) == 8 ? reinterpret_cast<const T *>(a.hii) : reinterpret_cast<const T *>(a.hii32);
@@ -789,7 +795,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
       hv.load(hsrc + idx);
 #pragma unroll
       for (int i = 0; i < VW; i++)
-        ov.v[i] = (T)((double)acc[r][g][i] + 0.5 * (((double)hv.v[i] + hshift) * (double)xo.v[i]));
+        ov.v[i] = (T)((double)acc[r][g][i] + 0.5 * __dmul_rn((double)hv.v[i] + hshift, (double)xo.v[i]));
       ov.store(out + idx);
     }
   }
@@ -853,8 +859,27 @@ int launch_pass_cm(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T
   return SBD_TPB_OK;
 }
 
+// Launch shapes of the general passes.  16-byte rows without the alpha-single x beta-single terms
+// take sigma_pass_cm_kernel; from a sweep (CUDA events, ms at 4e8 / 1e8 determinants, row groups /
+// CTAs per SM / column groups, "os": own values parked in shared memory), all giving the same bits:
+// FP32 alpha 2/7/2/os 3.10 / 1.31, 2/8/1/os 3.05 / 1.39, 2/8/2 3.19 / 1.30, 2/6/2 3.25 / 1.29, 2/8/2/os
+// 3.58 / 1.33; FP32 beta 2/8/2 2.78 / 1.18, 2/7/2 2.92 / 1.22, 2/6/2 3.09 / 1.27, 4/8/2 8.67 / 2.23;
+// FP64 alpha 2/7/2 5.52 / 2.18, 2/8/2 5.79 / 2.27, 2/6/2 5.97 / 2.33; FP64 beta 2/7/2 5.24 / 2.12, 2/8/2
+// 5.31 / 2.15, 2/6/2 5.63 / 2.25, 2/9/2 5.82 / 3.06 -- against sigma_block_kernel's 3.31 / 1.45,
+// 3.35 / 1.36, 6.38 / 2.52 and 5.76 / 2.71.  Other rows take sigma_block_kernel: FP32 alpha one row
+// group per thread below 10,000 CTAs (norb=12 FCI 0.84 -> 0.48 ms with two groups above), the values
+// for C^T parked in shared memory above.
 template <typename T, bool kAlpha>
 int launch_block(sbd_tpb_handle *h, const BlockArgs &ba, const T *X, T *out, T *XT) {
+  constexpr int VW = 16 / sizeof(T);
+  const bool rows16 = (ba.ncols % VW) == 0 && reinterpret_cast<uintptr_t>(X) % 16 == 0 &&
+                      reinterpret_cast<uintptr_t>(out) % 16 == 0 && (!XT || reinterpret_cast<uintptr_t>(XT) % 16 == 0);
+  if (rows16 && !ba.do_ab) {
+    if constexpr (sizeof(T) == 4 && kAlpha) return launch_pass_cm<T, true, 2, 7, 2, true>(h, ba, X, out, XT);
+    else if constexpr (sizeof(T) == 4) return launch_pass_cm<T, false, 2, 8, 2>(h, ba, X, out, XT);
+    else if constexpr (kAlpha) return launch_pass_cm<T, true, 2, 7, 2>(h, ba, X, out, XT);
+    else return launch_pass_cm<T, false, 2, 7, 2>(h, ba, X, out, XT);
+  }
   if constexpr (sizeof(T) == 4 && kAlpha) {
     const size_t blocks_g1 =
         ((ba.nrows + kBlkRows - 1) / kBlkRows) * ((ba.ncols + kBlkThreads * 4 - 1) / (kBlkThreads * 4));
