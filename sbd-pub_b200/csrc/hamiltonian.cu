@@ -263,6 +263,9 @@ void free_device_problem(sbd_tpb_handle *h) {
   free_dev(h->d_ab_kets);
   h->ab_nkets = 0;
   h->ab_nrows = h->ab_ncols = h->ab_max_k = 0;
+  h->ab_nchunks = 1;
+  h->ab_chunk = 0;
+  h->ab_dense = false;
   h->blk_for = nullptr;
   h->have_tables = false;
 }

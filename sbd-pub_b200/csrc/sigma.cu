@@ -372,11 +372,14 @@ __global__ void __launch_bounds__(kBlkThreads, M)
 //   sigma[Ia, Ib] += sum_{(Ja, pq, sa) in S_a(Ia)} sum_{(Jb, rs, sb) in S_b(Ib)} sa sb (pq|rs) C[Ja, Jb]
 // One CTA per alpha row Ia that has singles.  For a group of its singles the CTA stages in shared
 // memory the ket rows C[Ja] -- only the columns Jb that are kets of some beta single, compacted
-// (kets[] lists them ascending; the beta program addresses them by position) -- and the integral
-// rows sa (pq|.) (sign folded in), so the scattered reads C[Ja, Jb] and (pq|rs) at the beta singles
-// are shared-memory reads; each thread
-// owns a set of beta columns Ib that have singles and adds its sum into sigma[Ia, Ib] once per
-// group.  Groups are sized so several CTAs fit on an SM.  Without room for one row (kStage
+// (kets[] lists them ascending; the beta program addresses them by position), and of those one
+// range at a time -- and the integral rows sa (pq|.) (sign folded in), so the scattered reads
+// C[Ja, Jb] and (pq|rs) at the beta singles are shared-memory reads; each thread owns a set of beta
+// columns Ib that have singles and adds its sum over the range's entries into sigma[Ia, Ib] once
+// per group.  Every group re-reads the beta program's part for its range, so the ranges are made
+// short enough (on dense singles) for groups of several singles at two CTAs per SM; with sparse
+// singles there is one range and four CTAs per SM.  Sums in the vector type (FP32 vectors: FP32
+// products and sums, like the other FP32 sigma terms).  Without room for one staged row (kStage
 // false) the same loop reads C and the integrals through L1/L2.
 struct AbSparseArgs {
   const uint32_t *rows;  // alpha rows with at least one single
@@ -385,6 +388,7 @@ struct AbSparseArgs {
   const uint32_t *kets;  // [nk] the distinct kets of the beta singles, ascending
   uint32_t nk;
   uint32_t ncols_s;
+  uint32_t nchunks, chunk;  // ket ranges (program parts) and kets per range
   const uint32_t *as_off, *as_ket;
   const int32_t *as_pair;  // +-(pq + 1), sign = alpha sign
   const double *eri;       // (pq|rs) [L*L][L*L]
@@ -394,23 +398,27 @@ struct AbSparseArgs {
   double scale;    // weight of the term (1; 1/2 before the symmetric sigma's transpose-add)
 };
 
-template <typename T, bool kStage>
+template <typename T, bool kStage, bool kRanges>
 __global__ void __launch_bounds__(256)
     ab_sparse_kernel(AbSparseArgs a, const T *__restrict__ C, T *__restrict__ sigma) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *rows = reinterpret_cast<T *>(smem_raw);                // [group][nk]
-  T *gint = rows + (size_t)a.group * a.nk;                  // [group][L2], sign folded in
+  T *rows = reinterpret_cast<T *>(smem_raw);                // [group][chunk]
+  T *gint = rows + (size_t)a.group * a.chunk;               // [group][L2], sign folded in
   const uint32_t ia = __ldg(&a.rows[blockIdx.x]);
   const uint32_t e0 = __ldg(&a.as_off[ia]), e1 = __ldg(&a.as_off[ia + 1]);
   T *srow = sigma + (size_t)ia * a.nb;
+  const uint32_t nchunks = kRanges ? a.nchunks : 1;
+  for (uint32_t m = 0; m < nchunks; m++) {
+  const uint32_t k0 = kRanges ? m * a.chunk : 0, nkm = kRanges ? min(a.nk, k0 + a.chunk) - k0 : a.nk;
+  const uint2 *colp = kRanges ? a.colp + (size_t)m * (a.ncols_s + 1) : a.colp;
   for (uint32_t g0 = e0; g0 < e1; g0 += a.group) {
     const uint32_t g1 = min(e1, g0 + a.group), ng = g1 - g0;
     if (kStage) {
       __syncthreads();
       for (uint32_t j = 0; j < ng; j++) {
         const T *src = C + (size_t)__ldg(&a.as_ket[g0 + j]) * a.nb;
-        T *dst = rows + (size_t)j * a.nk;
-        for (uint32_t c = threadIdx.x; c < a.nk; c += blockDim.x) dst[c] = __ldg(&src[__ldg(&a.kets[c])]);
+        T *dst = rows + (size_t)j * a.chunk;
+        for (uint32_t c = threadIdx.x; c < nkm; c += blockDim.x) dst[c] = __ldg(&src[__ldg(&a.kets[k0 + c])]);
         const int32_t pa = __ldg(&a.as_pair[g0 + j]);
         const double *erow = a.eri + (size_t)((pa > 0 ? pa : -pa) - 1) * a.L2;
         T *gdst = gint + (size_t)j * a.L2;
@@ -421,45 +429,48 @@ __global__ void __launch_bounds__(256)
       }
       __syncthreads();
     }
-    // sum over the beta singles of compact column q (its column index in ib)
-    auto column = [&](uint32_t q, uint32_t &ib) -> double {
-      const uint2 c0 = __ldg(&a.colp[q]), c1 = __ldg(&a.colp[q + 1]);
+    // sum over the beta singles of compact column q in this ket range (its column index in ib;
+    // false when the range has none of them)
+    auto column = [&](uint32_t q, uint32_t &ib, double &out) -> bool {
+      const uint2 c0 = __ldg(&colp[q]), c1 = __ldg(&colp[q + 1]);
       ib = c0.x;
-      double acc = 0.0;
+      T acc = 0;
       for (uint32_t f = c0.y; f < c1.y; f++) {
         const uint2 be = __ldg(&a.bsp[f]);
-        const uint32_t jb = be.x;
+        const uint32_t jb = be.x - k0;
         const int32_t pb = (int32_t)be.y;
         const int rs = (pb > 0 ? pb : -pb) - 1;
-        double sum = 0.0;
+        T sum = 0;
         for (uint32_t j = 0; j < ng; j++) {
           if (kStage) {
-            sum += (double)gint[(size_t)j * a.L2 + rs] * (double)rows[(size_t)j * a.nk + jb];
+            sum = madd(sum, gint[(size_t)j * a.L2 + rs], rows[(size_t)j * a.chunk + jb]);
           } else {
             const int32_t pa = __ldg(&a.as_pair[g0 + j]);
-            const double g = __ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
-            sum += (pa > 0 ? g : -g) *
-                   (double)__ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + __ldg(&a.kets[jb])]);
+            const T g = (T)__ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
+            sum = madd(sum, pa > 0 ? g : -g, __ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + __ldg(&a.kets[be.x])]));
           }
         }
         acc += pb > 0 ? sum : -sum;
       }
-      return acc;
+      out = (double)acc;
+      return !kRanges || c1.y > c0.y;
     };
     // two independent columns per iteration, so their load chains overlap
     uint32_t q = threadIdx.x;
     for (; q + blockDim.x < a.ncols_s; q += 2 * blockDim.x) {
       uint32_t ib0, ib1;
-      const double s0 = column(q, ib0), s1 = column(q + blockDim.x, ib1);
-      const T o0 = srow[ib0], o1 = srow[ib1];
-      srow[ib0] = (T)((double)o0 + a.scale * s0);
-      srow[ib1] = (T)((double)o1 + a.scale * s1);
+      double s0, s1;
+      const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
+      const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);  // both loads before the stores
+      if (h0) srow[ib0] = (T)((double)o0 + a.scale * s0);
+      if (h1) srow[ib1] = (T)((double)o1 + a.scale * s1);
     }
     if (q < a.ncols_s) {
       uint32_t ib0;
-      const double s0 = column(q, ib0);
-      srow[ib0] = (T)((double)srow[ib0] + a.scale * s0);
+      double s0;
+      if (column(q, ib0, s0)) srow[ib0] = (T)((double)srow[ib0] + a.scale * s0);
     }
+  }
   }
 }
 
@@ -999,24 +1010,40 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
     std::stable_sort(cols.begin(), cols.end(), [&](uint32_t x, uint32_t y) {
       return bo[x + 1] - bo[x] > bo[y + 1] - bo[y];
     });
-    std::vector<uint2> colp, bsp(std::max<size_t>(1, nnz));
-    std::vector<uint32_t> eorder;  // entry of the original table at each packed position
-    eorder.reserve(nnz);
-    for (const uint32_t c : cols) {
-      colp.push_back(make_uint2(c, (uint32_t)eorder.size()));
-      for (uint32_t f = bo[c]; f < bo[c + 1]; f++) eorder.push_back(f);
-    }
-    const size_t ncs = colp.size();
-    colp.push_back(make_uint2(0u, (uint32_t)nnz));
     // the distinct kets of the beta singles, and each entry's ket as its position among them
     std::vector<uint32_t> kets(bket.begin(), bket.begin() + nnz);
     std::sort(kets.begin(), kets.end());
     kets.erase(std::unique(kets.begin(), kets.end()), kets.end());
-    for (size_t i = 0; i < nnz; i++) {
-      const uint32_t f = eorder[i];
-      const uint32_t pos = (uint32_t)(std::lower_bound(kets.begin(), kets.end(), bket[f]) - kets.begin());
-      bsp[i] = make_uint2(pos, (uint32_t)bpair[f]);
+    std::vector<uint32_t> kpos(std::max<size_t>(1, nnz));
+    for (size_t f = 0; f < nnz; f++)
+      kpos[f] = (uint32_t)(std::lower_bound(kets.begin(), kets.end(), bket[f]) - kets.begin());
+    // Ket ranges: the kernel stages, per group of alpha singles, their C rows restricted to one
+    // range of the kets, and every group re-reads the part of the beta program for that range.
+    // With dense beta singles (more than 4 entries per distinct ket: the program is then many
+    // times the bytes of a staged row) and more singles per row than one group holds at four CTAs
+    // per SM, the fewest ranges that let a group hold min(8, most singles of a row) singles at two
+    // CTAs per SM in FP64 (FP32 then holds twice as many); else one range.
+    const size_t nk = kets.size(), L2 = (size_t)h->L * h->L;
+    const size_t b4 = h->smem_optin / 4 - 1024, b2 = h->smem_optin / 2 - 1024;
+    uint32_t nch = 1;
+    const bool dense = nk > 0 && nnz > 4 * nk;
+    if (dense && b4 / ((nk + L2) * sizeof(double)) < kmax) {
+      const size_t want = std::min<size_t>(8, kmax);
+      while (nch < 64 && b2 / (((nk + nch - 1) / nch + L2) * sizeof(double)) < want) nch++;
     }
+    const uint32_t chunk = nk > 0 ? (uint32_t)((nk + nch - 1) / nch) : 1;
+    // program: per range, per column (most singles first) its entries in that range, in table order
+    std::vector<uint2> colp, bsp(std::max<size_t>(1, nnz));
+    size_t w = 0;
+    for (uint32_t m = 0; m < nch; m++) {
+      for (const uint32_t c : cols) {
+        colp.push_back(make_uint2(c, (uint32_t)w));
+        for (uint32_t f = bo[c]; f < bo[c + 1]; f++)
+          if (kpos[f] / chunk == m) bsp[w++] = make_uint2(kpos[f], (uint32_t)bpair[f]);
+      }
+      colp.push_back(make_uint2(0u, (uint32_t)w));
+    }
+    const size_t ncs = cols.size();
     if (kets.empty()) kets.push_back(0);
     TPB_CUDA(cudaMalloc(&h->d_ab_rows, sizeof(uint32_t) * std::max<size_t>(1, rows.size())));
     TPB_CUDA(cudaMalloc(&h->d_ab_colp, sizeof(uint2) * colp.size()));
@@ -1031,6 +1058,9 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
     h->ab_nrows = (uint32_t)rows.size();
     h->ab_ncols = (uint32_t)ncs;
     h->ab_max_k = kmax;
+    h->ab_nchunks = nch;
+    h->ab_chunk = chunk;
+    h->ab_dense = dense;
   }
   return SBD_TPB_OK;
 }
@@ -1046,25 +1076,33 @@ int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma, double scale = 1.0
   a.kets = h->d_ab_kets;
   a.nk = h->ab_nkets;
   a.ncols_s = h->ab_ncols;
+  a.nchunks = h->ab_nchunks;
+  a.chunk = h->ab_chunk;
   a.as_off = h->ta_s.off;
   a.as_ket = h->ta_s.ket;
   a.as_pair = h->pa.s_pair;
   a.eri = h->d_eri;
   a.L2 = h->L * h->L;
   a.nb = (uint32_t)h->bstr.size();
-  // one staged single = its compacted C row and its integral row; aim for 4 CTAs per SM, else as
-  // many singles as fit in one CTA's shared memory
-  const size_t per = ((size_t)a.nk + a.L2) * sizeof(T);
-  const size_t target = std::max<size_t>(per, h->smem_optin / 4 - 1024);
+  // one staged single = its C row over one ket range and its integral row; with a dense beta
+  // program (each group re-reads its range's part) the largest group that leaves 2 CTAs per SM,
+  // else groups sized for 4 CTAs per SM.  Measured, ab term ms at the previous one range and 4 CTAs
+  // -> ranges and 2 CTAs: norb=18 / 8.7e7 determinants (51 singles per string) FP32 875 -> 310,
+  // FP64 825 -> 517; norb=24 / 1.9e8 (63 per string) FP32 2915 -> 1167, FP64 5270 -> 2070;
+  // norb=24 / 3.0e7 FP32 162 -> 117, FP64 322 -> 191.  Sparse singles (norb=28-32 selected sets)
+  // keep one range and 4 CTAs per SM: 2 CTAs took them from 0.71 to 1.1-1.2 ms (FP32).
+  const size_t per = ((size_t)a.chunk + a.L2) * sizeof(T);
+  const size_t target = std::max<size_t>(per, h->smem_optin / (h->ab_dense ? 2 : 4) - 1024);
   if (per <= h->smem_optin) {
     a.group = (uint32_t)std::max<size_t>(1, std::min<size_t>(target / per, h->ab_max_k));
     const size_t smem = a.group * per;
-    TPB_CUDA(cudaFuncSetAttribute(ab_sparse_kernel<T, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ab_sparse_kernel<T, true><<<h->ab_nrows, 256, smem, h->stream>>>(a, C, sigma);
+    const auto kern = a.nchunks > 1 ? ab_sparse_kernel<T, true, true> : ab_sparse_kernel<T, true, false>;
+    TPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<h->ab_nrows, 256, smem, h->stream>>>(a, C, sigma);
   } else {
     a.group = h->ab_max_k;
-    ab_sparse_kernel<T, false><<<h->ab_nrows, 256, 0, h->stream>>>(a, C, sigma);
+    const auto kern = a.nchunks > 1 ? ab_sparse_kernel<T, false, true> : ab_sparse_kernel<T, false, false>;
+    kern<<<h->ab_nrows, 256, 0, h->stream>>>(a, C, sigma);
   }
   TPB_LAUNCHED(h);
   return SBD_TPB_OK;

@@ -182,11 +182,13 @@ struct sbd_tpb_handle {
   size_t ab_work_bytes = 0;
   // sparse alpha-beta term: alpha rows and beta columns that have at least one single
   uint32_t *d_ab_rows = nullptr;
-  uint2 *d_ab_colp = nullptr;  // per beta column with singles, most singles first: (column, first entry); last: (0, nnz)
+  uint2 *d_ab_colp = nullptr;  // per ket range, per beta column with singles (most singles first): (column, first entry); then (0, end of the range's entries)
   uint2 *d_ab_bsp = nullptr;   // beta singles entries packed as (ket position in d_ab_kets, signed pair label)
   uint32_t *d_ab_kets = nullptr;  // distinct kets of the beta singles, ascending
   uint32_t ab_nkets = 0;
   uint32_t ab_nrows = 0, ab_ncols = 0, ab_max_k = 0;  // ab_max_k: most singles of one alpha row
+  uint32_t ab_nchunks = 1, ab_chunk = 0;              // ket ranges of the beta program, kets per range
+  bool ab_dense = false;                              // beta program of more than 4 entries per ket
   // learned preconditioner attached by sbd_tpb_set_preconditioner (not owned) and the
   // occupation windows of the strings it reads
   struct sbd_tpb_precond *precond = nullptr;

@@ -7,8 +7,8 @@ h2o_1em3 / n2_1em3 fixtures (the same FCIDUMP files).  FP64 solves must land wit
 published value (its rounding is 5e-9); mixed-precision solves within 1e-6 Ha.
 
 The h2o sets above 1e-5 are dense (25,062 of the 42,504 possible strings at 1e-7, about a thousand
-doubles per string), so their solves take minutes on one B200 (1e-6 FP64 113 s, 1e-6 mixed 55 s,
-1e-7 mixed 399 s); they run only with SBD_TPB_LONG_TESTS=1."""
+doubles per string), so their solves take a minute or more on one B200 (1e-6 FP64 113 s, 1e-6 mixed
+55 s, 1e-7 mixed 399 s); the 1e-7 set (6.3e8 determinants) runs only with SBD_TPB_LONG_TESTS=1."""
 import os
 
 import numpy as np
@@ -76,7 +76,7 @@ LONG = pytest.mark.skipif(os.environ.get("SBD_TPB_LONG_TESTS") != "1",
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["n2_3em4", "n2_1em4", "n2_1em5", "n2_1em6", "h2o_1em4", "h2o_1em5",
-                                  pytest.param("h2o_1em6", marks=LONG)])
+                                  "h2o_1em6"])
 def test_gpu_published_energy_fp64(name):
     import sbd_tpb
     prob, meta = published_problem(name)
@@ -86,10 +86,9 @@ def test_gpu_published_energy_fp64(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["h2o_1em5", pytest.param("h2o_1em6", marks=LONG),
-                                  pytest.param("h2o_1em7", marks=LONG)])
+@pytest.mark.parametrize("name", ["h2o_1em5", "h2o_1em6", pytest.param("h2o_1em7", marks=LONG)])
 def test_gpu_published_energy_mixed(name):
-    """FP32 vectors, FP64 projections and a final FP64 sigma (3.0e7 determinants; 1.9e8 and 6.3e8 with
+    """FP32 vectors, FP64 projections and a final FP64 sigma (3.0e7 and 1.9e8 determinants; 6.3e8 with
     SBD_TPB_LONG_TESTS=1)."""
     import sbd_tpb
     prob, meta = published_problem(name)
