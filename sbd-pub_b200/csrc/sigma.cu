@@ -395,7 +395,8 @@ struct AbSparseArgs {
   int L2;
   uint32_t nb;     // row length of C and sigma
   uint32_t group;  // singles staged per round
-  double scale;    // weight of the term (1; 1/2 before the symmetric sigma's transpose-add)
+  double scale;    // weight of the term
+  int upper;       // only columns Ib >= Ia (weight 1/2 on Ib == Ia): the symmetric sigma's B
 };
 
 template <typename T, bool kStage, bool kRanges>
@@ -460,15 +461,33 @@ __global__ void __launch_bounds__(256)
     for (; q + blockDim.x < a.ncols_s; q += 2 * blockDim.x) {
       uint32_t ib0, ib1;
       double s0, s1;
+      if (a.upper) {
+        // the symmetric sigma's B: columns Ib >= Ia only (B + B^T restores the rest), the diagonal
+        // at half weight
+        const uint32_t c0 = __ldg(&colp[q]).x, c1 = __ldg(&colp[q + blockDim.x]).x;
+        const bool u0 = c0 >= ia, u1 = c1 >= ia;
+        if (!u0 && !u1) continue;
+        if (u0 && u1) {
+          const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
+          const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);
+          if (h0) srow[ib0] = (T)((double)o0 + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+          if (h1) srow[ib1] = (T)((double)o1 + (ib1 == ia ? 0.5 : 1.0) * a.scale * s1);
+        } else {
+          const uint32_t qq = u0 ? q : q + blockDim.x;
+          if (column(qq, ib0, s0)) srow[ib0] = (T)((double)srow[ib0] + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+        }
+        continue;
+      }
       const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
       const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);  // both loads before the stores
       if (h0) srow[ib0] = (T)((double)o0 + a.scale * s0);
       if (h1) srow[ib1] = (T)((double)o1 + a.scale * s1);
     }
-    if (q < a.ncols_s) {
+    if (q < a.ncols_s && (!a.upper || __ldg(&colp[q]).x >= ia)) {
       uint32_t ib0;
       double s0;
-      if (column(q, ib0, s0)) srow[ib0] = (T)((double)srow[ib0] + a.scale * s0);
+      if (column(q, ib0, s0))
+        srow[ib0] = (T)((double)srow[ib0] + (a.upper && ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
     }
   }
   }
@@ -1066,10 +1085,11 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
 }
 
 template <typename T>
-int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma, double scale = 1.0) {
+int launch_ab_sparse(sbd_tpb_handle *h, const T *C, T *sigma, double scale = 1.0, bool upper = false) {
   if (h->ab_nrows == 0 || h->ab_ncols == 0) return SBD_TPB_OK;
   AbSparseArgs a{};
   a.scale = scale;
+  a.upper = upper ? 1 : 0;
   a.rows = h->d_ab_rows;
   a.colp = h->d_ab_colp;
   a.bsp = h->d_ab_bsp;
@@ -1241,7 +1261,7 @@ int sigma_sep_sym(sbd_tpb_handle *h, const T *C, T *sigma, double shift, const T
   if (dense_ab) {
     TPB_CHECK(ab_dense_apply<T>(h, C, sigma, 0.5));
   } else {
-    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma, 0.5));
+    TPB_CHECK(launch_ab_sparse<T>(h, C, sigma, 1.0, true));
   }
   TPB_CUDA(cudaEventRecord(h->ev_k[1], h->stream));
   if (m > 0) TPB_CHECK(sym_add_dots<T>(h, sigma, S, m, slot));
