@@ -95,3 +95,45 @@ def test_gpu_published_energy_mixed(name):
     r = _solve(prob, sbd_tpb.MIXED, 1e-5)
     assert r["converged"]
     assert r["energy"] == pytest.approx(meta["published"], abs=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_sigma_dense_singles(oracle):
+    """Sigma where the alpha-beta kernel's beta program is split by ket range (dense beta singles: n2 1e-5,
+    4,041 strings, 1.6e7 determinants, ~48 singles per string): the general form equals the oracle's
+    sigma (orc_sigma_rows, the reference's convention and per-element order) at 200 sampled determinants,
+    FP64 within 1e-12 and FP32 within 2e-5 of the largest sampled |sigma|; and the exchange-symmetric
+    form (its alpha-beta term on the upper triangle only) equals the general form on a symmetric vector
+    (FP64 1e-13, FP32 3e-6 of the largest |sigma|)."""
+    import torch
+
+    import sbd_tpb
+    from test_large_configs import _hash_vector_device
+    prob, meta = published_problem("n2_1em5")
+    h = sbd_tpb.Handle(0)
+    h.set_problem(prob)
+    rows = np.random.default_rng(6).choice(prob.ndet, size=200, replace=False)
+    ham = oracle.Hamiltonian.from_arrays(prob.norb, prob.nelec, prob.core, prob.h1, prob.eri_packed)
+    ref = oracle.System(ham, prob.astr, prob.bstr).sigma_rows(rows)  # closed-form hash vector
+    scale = float(np.max(np.abs(ref)))
+    idx = torch.from_numpy(rows.astype(np.int64)).cuda()
+    x64 = _hash_vector_device(prob.ndet)
+    for x, tol in ((x64, 1e-12), (x64.float(), 2e-5)):
+        y = torch.empty_like(x)
+        h.sigma_device(x, y, separated=False)
+        assert np.max(np.abs(y[idx].double().cpu().numpy() - ref)) <= tol * scale, (x.dtype, tol)
+        del y
+    del x64
+    n = len(prob.astr)
+    g = torch.Generator(device="cuda").manual_seed(8)
+    r = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    xs = ((r + r.T) * 0.5).reshape(-1).contiguous()
+    del r
+    for x, tol in ((xs, 1e-13), (xs.float(), 3e-6)):
+        gen, sym = torch.empty_like(x), torch.empty_like(x)
+        h.sigma_device(x, gen)
+        h.sigma_device(x, sym, symmetric=True)
+        err = float((sym.double() - gen.double()).abs().max()) / float(gen.double().abs().max())
+        assert err <= tol, (x.dtype, err)
+        del gen, sym
+    h.close()
