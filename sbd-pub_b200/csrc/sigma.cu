@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kBlkThreads, M)
 // false) the same loop reads C and the integrals through L1/L2.
 struct AbSparseArgs {
   const uint32_t *rows;  // alpha rows with at least one single
-  const uint2 *colp;     // beta columns with singles: (column, first entry), then (0, nnz)
+  const uint2 *colp;     // per ket range: (column, first entry) of each beta column with singles, then (0, range end)
   const uint2 *bsp;      // beta singles entries: (position of the ket in kets, +-(rs + 1) with the beta sign)
   const uint32_t *kets;  // [nk] the distinct kets of the beta singles, ascending
   uint32_t nk;
