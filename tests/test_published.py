@@ -100,7 +100,7 @@ def test_gpu_published_energy_mixed(name):
 @pytest.mark.gpu
 def test_gpu_sigma_dense_singles(oracle):
     """Sigma where the alpha-beta kernel's beta program is split by ket range (dense beta singles: n2 1e-5,
-    4,041 strings, 1.6e7 determinants, ~48 singles per string): the general form equals the oracle's
+    4,041 strings, 1.6e7 determinants, tens of singles per string): the general form equals the oracle's
     sigma (orc_sigma_rows, the reference's convention and per-element order) at 200 sampled determinants,
     FP64 within 1e-12 and FP32 within 2e-5 of the largest sampled |sigma|; and the exchange-symmetric
     form (its alpha-beta term on the upper triangle only) equals the general form on a symmetric vector
