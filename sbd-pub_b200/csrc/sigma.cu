@@ -1043,7 +1043,8 @@ int prepare_sigma_meta(sbd_tpb_handle *h, bool want_ab_lists) {
     // per SM, the fewest ranges that let a group hold min(8, most singles of a row) singles at two
     // CTAs per SM in FP64 (FP32 then holds twice as many); else one range.  Targets of 12, 16 and 24
     // singles per group (more, shorter ranges) measured slower: norb=18 / 8.7e7 determinants FP64
-    // 510 -> 520 / 563 / 699 ms, norb=24 / 3.0e7 189 -> 213 / 261 / 774 ms.
+    // 510 -> 520 / 563 / 699 ms, norb=24 / 3.0e7 189 -> 213 / 261 / 774 ms; targets of 4 and 6 were within
+    // 1 % of 8 there (FP64), FP32 norb=24 105 / 113 against 114 ms.
     const size_t nk = kets.size(), L2 = (size_t)h->L * h->L;
     const size_t b4 = h->smem_optin / 4 - 1024, b2 = h->smem_optin / 2 - 1024;
     uint32_t nch = 1;
