@@ -410,86 +410,86 @@ __global__ void __launch_bounds__(256)
   T *srow = sigma + (size_t)ia * a.nb;
   const uint32_t nchunks = kRanges ? a.nchunks : 1;
   for (uint32_t m = 0; m < nchunks; m++) {
-  const uint32_t k0 = kRanges ? m * a.chunk : 0, nkm = kRanges ? min(a.nk, k0 + a.chunk) - k0 : a.nk;
-  const uint2 *colp = kRanges ? a.colp + (size_t)m * (a.ncols_s + 1) : a.colp;
-  for (uint32_t g0 = e0; g0 < e1; g0 += a.group) {
-    const uint32_t g1 = min(e1, g0 + a.group), ng = g1 - g0;
-    if (kStage) {
-      __syncthreads();
-      for (uint32_t j = 0; j < ng; j++) {
-        const T *src = C + (size_t)__ldg(&a.as_ket[g0 + j]) * a.nb;
-        T *dst = rows + (size_t)j * a.chunk;
-        for (uint32_t c = threadIdx.x; c < nkm; c += blockDim.x) dst[c] = __ldg(&src[__ldg(&a.kets[k0 + c])]);
-        const int32_t pa = __ldg(&a.as_pair[g0 + j]);
-        const double *erow = a.eri + (size_t)((pa > 0 ? pa : -pa) - 1) * a.L2;
-        T *gdst = gint + (size_t)j * a.L2;
-        for (int c = threadIdx.x; c < a.L2; c += blockDim.x) {
-          const double g = __ldg(&erow[c]);
-          gdst[c] = (T)(pa > 0 ? g : -g);
-        }
-      }
-      __syncthreads();
-    }
-    // sum over the beta singles of compact column q in this ket range (its column index in ib;
-    // false when the range has none of them)
-    auto column = [&](uint32_t q, uint32_t &ib, double &out) -> bool {
-      const uint2 c0 = __ldg(&colp[q]), c1 = __ldg(&colp[q + 1]);
-      ib = c0.x;
-      T acc = 0;
-      for (uint32_t f = c0.y; f < c1.y; f++) {
-        const uint2 be = __ldg(&a.bsp[f]);
-        const uint32_t jb = be.x - k0;
-        const int32_t pb = (int32_t)be.y;
-        const int rs = (pb > 0 ? pb : -pb) - 1;
-        T sum = 0;
+    const uint32_t k0 = kRanges ? m * a.chunk : 0, nkm = kRanges ? min(a.nk, k0 + a.chunk) - k0 : a.nk;
+    const uint2 *colp = kRanges ? a.colp + (size_t)m * (a.ncols_s + 1) : a.colp;
+    for (uint32_t g0 = e0; g0 < e1; g0 += a.group) {
+      const uint32_t g1 = min(e1, g0 + a.group), ng = g1 - g0;
+      if (kStage) {
+        __syncthreads();
         for (uint32_t j = 0; j < ng; j++) {
-          if (kStage) {
-            sum = madd(sum, gint[(size_t)j * a.L2 + rs], rows[(size_t)j * a.chunk + jb]);
-          } else {
-            const int32_t pa = __ldg(&a.as_pair[g0 + j]);
-            const T g = (T)__ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
-            sum = madd(sum, pa > 0 ? g : -g, __ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + __ldg(&a.kets[be.x])]));
+          const T *src = C + (size_t)__ldg(&a.as_ket[g0 + j]) * a.nb;
+          T *dst = rows + (size_t)j * a.chunk;
+          for (uint32_t c = threadIdx.x; c < nkm; c += blockDim.x) dst[c] = __ldg(&src[__ldg(&a.kets[k0 + c])]);
+          const int32_t pa = __ldg(&a.as_pair[g0 + j]);
+          const double *erow = a.eri + (size_t)((pa > 0 ? pa : -pa) - 1) * a.L2;
+          T *gdst = gint + (size_t)j * a.L2;
+          for (int c = threadIdx.x; c < a.L2; c += blockDim.x) {
+            const double g = __ldg(&erow[c]);
+            gdst[c] = (T)(pa > 0 ? g : -g);
           }
         }
-        acc += pb > 0 ? sum : -sum;
+        __syncthreads();
       }
-      out = (double)acc;
-      return !kRanges || c1.y > c0.y;
-    };
-    // two independent columns per iteration, so their load chains overlap
-    uint32_t q = threadIdx.x;
-    for (; q + blockDim.x < a.ncols_s; q += 2 * blockDim.x) {
-      uint32_t ib0, ib1;
-      double s0, s1;
-      if (a.upper) {
-        // the symmetric sigma's B: columns Ib >= Ia only (B + B^T restores the rest), the diagonal
-        // at half weight
-        const uint32_t c0 = __ldg(&colp[q]).x, c1 = __ldg(&colp[q + blockDim.x]).x;
-        const bool u0 = c0 >= ia, u1 = c1 >= ia;
-        if (!u0 && !u1) continue;
-        if (u0 && u1) {
-          const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
-          const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);
-          if (h0) srow[ib0] = (T)((double)o0 + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
-          if (h1) srow[ib1] = (T)((double)o1 + (ib1 == ia ? 0.5 : 1.0) * a.scale * s1);
-        } else {
-          const uint32_t qq = u0 ? q : q + blockDim.x;
-          if (column(qq, ib0, s0)) srow[ib0] = (T)((double)srow[ib0] + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+      // sum over the beta singles of compact column q in this ket range (its column index in ib;
+      // false when the range has none of them)
+      auto column = [&](uint32_t q, uint32_t &ib, double &out) -> bool {
+        const uint2 c0 = __ldg(&colp[q]), c1 = __ldg(&colp[q + 1]);
+        ib = c0.x;
+        T acc = 0;
+        for (uint32_t f = c0.y; f < c1.y; f++) {
+          const uint2 be = __ldg(&a.bsp[f]);
+          const uint32_t jb = be.x - k0;
+          const int32_t pb = (int32_t)be.y;
+          const int rs = (pb > 0 ? pb : -pb) - 1;
+          T sum = 0;
+          for (uint32_t j = 0; j < ng; j++) {
+            if (kStage) {
+              sum = madd(sum, gint[(size_t)j * a.L2 + rs], rows[(size_t)j * a.chunk + jb]);
+            } else {
+              const int32_t pa = __ldg(&a.as_pair[g0 + j]);
+              const T g = (T)__ldg(&a.eri[(size_t)((pa > 0 ? pa : -pa) - 1) * a.L2 + rs]);
+              sum = madd(sum, pa > 0 ? g : -g, __ldg(&C[(size_t)__ldg(&a.as_ket[g0 + j]) * a.nb + __ldg(&a.kets[be.x])]));
+            }
+          }
+          acc += pb > 0 ? sum : -sum;
         }
-        continue;
+        out = (double)acc;
+        return !kRanges || c1.y > c0.y;
+      };
+      // two independent columns per iteration, so their load chains overlap
+      uint32_t q = threadIdx.x;
+      for (; q + blockDim.x < a.ncols_s; q += 2 * blockDim.x) {
+        uint32_t ib0, ib1;
+        double s0, s1;
+        if (a.upper) {
+          // the symmetric sigma's B: columns Ib >= Ia only (B + B^T restores the rest), the diagonal
+          // at half weight
+          const uint32_t c0 = __ldg(&colp[q]).x, c1 = __ldg(&colp[q + blockDim.x]).x;
+          const bool u0 = c0 >= ia, u1 = c1 >= ia;
+          if (!u0 && !u1) continue;
+          if (u0 && u1) {
+            const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
+            const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);
+            if (h0) srow[ib0] = (T)((double)o0 + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+            if (h1) srow[ib1] = (T)((double)o1 + (ib1 == ia ? 0.5 : 1.0) * a.scale * s1);
+          } else {
+            const uint32_t qq = u0 ? q : q + blockDim.x;
+            if (column(qq, ib0, s0)) srow[ib0] = (T)((double)srow[ib0] + (ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+          }
+          continue;
+        }
+        const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
+        const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);  // both loads before the stores
+        if (h0) srow[ib0] = (T)((double)o0 + a.scale * s0);
+        if (h1) srow[ib1] = (T)((double)o1 + a.scale * s1);
       }
-      const bool h0 = column(q, ib0, s0), h1 = column(q + blockDim.x, ib1, s1);
-      const T o0 = h0 ? srow[ib0] : T(0), o1 = h1 ? srow[ib1] : T(0);  // both loads before the stores
-      if (h0) srow[ib0] = (T)((double)o0 + a.scale * s0);
-      if (h1) srow[ib1] = (T)((double)o1 + a.scale * s1);
+      if (q < a.ncols_s && (!a.upper || __ldg(&colp[q]).x >= ia)) {
+        uint32_t ib0;
+        double s0;
+        if (column(q, ib0, s0))
+          srow[ib0] = (T)((double)srow[ib0] + (a.upper && ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
+      }
     }
-    if (q < a.ncols_s && (!a.upper || __ldg(&colp[q]).x >= ia)) {
-      uint32_t ib0;
-      double s0;
-      if (column(q, ib0, s0))
-        srow[ib0] = (T)((double)srow[ib0] + (a.upper && ib0 == ia ? 0.5 : 1.0) * a.scale * s0);
-    }
-  }
   }
 }
 
